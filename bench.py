@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark of the per-energy NEGF hot path on B200.
+
+Workload (one GPU): 32 diagonal blocks of 256x256, 1024 energies in
+[-3, 3] (complex128, FP64 arithmetic). One *energy point* = assembly of
+A(E), both-contact Sancho-Rubio OBC to 1e-12 with the OBCSystem refinement
+step and the boundary self-energies, RGF selected solve (G^R diagonal,
+G^< and G^> diagonal + off-diagonal blocks, Meir-Wingreen current), Caroli
+transmission and density. A *step* is one batch of energies
+(default 128); steps cycle through the energy grid, which is split evenly
+across ranks (independent energies: weak scaling, no collective in the
+data path).
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]``
+prints one JSON line on rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "RGF energy-points/s at 256x256 blocks (FP64)"
+UNIT = "energy-points/s"
+WORKLOAD = ("32 blocks of 256x256, 1024 energies in [-3,3], complex128: both-contact Sancho-Rubio "
+            "(tol 1e-12) + OBC refinement + selected_solve (G^R, G^<, G^>, current) + Caroli "
+            "transmission + density per energy point")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=8)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--batch", type=int, default=128)
+    p.add_argument("--energies", type=int, default=1024)
+    p.add_argument("--e2e-batch", type=int, default=8)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-energies", type=int, default=2)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", self.gpu_id], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_fp64_peak(torch, device) -> dict:
+    """cuBLAS FP64 throughput on this GPU (best of 5): DGEMM 8192^3 and
+    ZGEMM 4096^3; the larger figure is the FP64 roofline denominator."""
+    res = {}
+    for name, dtype, n, per in (("dgemm", torch.float64, 8192, 2.0), ("zgemm", torch.complex128, 4096, 8.0)):
+        a = torch.randn((n, n), dtype=dtype, device=device)
+        b = torch.randn((n, n), dtype=dtype, device=device)
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        res[name] = per * n ** 3 / (best * 1e-3) / 1e12
+        del a, b
+    torch.cuda.empty_cache()
+    res["peak"] = max(res["dgemm"], res["zgemm"])
+    return res
+
+
+def cpu_baseline(num: int) -> dict:
+    """The oracle (NumPy restatement of the reference path) on a bounded
+    sample of the workload, all host cores."""
+    from oracle import negf_oracle as o
+    from quatrex_b200 import synthetic
+
+    dev = synthetic.cfg1()
+    idx = np.linspace(100, 900, num).astype(int)
+    e = dev.energies[idx]
+    diag, upper, lower = dev.system_blocks(e)
+    t0 = time.perf_counter()
+    o.energy_point_solve(diag, upper, lower, dev.fermi_left(e), dev.fermi_right(e))
+    dt = time.perf_counter() - t0
+    return {"value": num / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{num} energies of the 1024-point grid (indices {idx.tolist()}), one batch",
+            "seconds": dt, "blas_threads": _blas_threads()}
+
+
+def _blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        return [d.get("num_threads") for d in threadpool_info()]
+    except Exception:  # noqa: BLE001 - informational only
+        return None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import negf_oracle as o
+    from quatrex_b200 import synthetic
+
+    dev = synthetic.cfg1(args.energies)
+    times = []
+    for step in range(args.warmup + args.steps):
+        i = (137 * step + 11) % args.energies
+        e = dev.energies[i:i + 1]
+        diag, upper, lower = dev.system_blocks(e)
+        t0 = time.perf_counter()
+        o.energy_point_solve(diag, upper, lower, dev.fermi_left(e), dev.fermi_right(e))
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "step": "1 energy point per step (bounded CPU sample)",
+                   "parallelism": "host BLAS threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{len(times)} single-energy steps of the 1024-point grid",
+                         "blas_threads": _blas_threads()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def e2e_leg(torch, device, dev, energies, steps):
+    """The reference-facing plugin path with pinned HOST buffers: the caller's
+    DSDBCOO stacks live in host memory; OBCSystem(SanchoRubio) and
+    RGF.selected_solve copy them in and the results out in every step."""
+    import scipy.sparse as sps
+
+    from quatrex_b200 import RGF, DSDBCOO, OBCBlocks, OBCSystem, SanchoRubio, contact_self_energy
+    from quatrex_b200 import observables
+
+    n, b = dev.num_blocks, dev.block_size
+    B = energies.size
+    rows, cols = [], []
+    for i in range(n):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < n:
+                r, c = np.meshgrid(np.arange(b) + i * b, np.arange(b) + j * b, indexing="ij")
+                rows.append(r.ravel())
+                cols.append(c.ravel())
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    pattern = sps.coo_matrix((np.ones(rows.size, dtype=np.complex128), (rows, cols)), shape=(n * b, n * b))
+    proto = DSDBCOO.from_sparray(pattern, dev.block_sizes, (1,))
+
+    def host(m=None):
+        d = torch.zeros((B, proto.nnz), dtype=torch.complex128).pin_memory()
+        return DSDBCOO(d, proto.rows, proto.cols, proto.block_sizes, _layout=proto._layout)
+
+    A, SL, SG, XL, XG, XR = (host() for _ in range(6))
+    diag, upper, lower = dev.system_blocks(energies)
+    for i in range(n):
+        A.blocks[i, i] = torch.from_numpy(diag[i])
+        if i + 1 < n:
+            A.blocks[i, i + 1] = torch.from_numpy(upper[i])
+            A.blocks[i + 1, i] = torch.from_numpy(lower[i])
+    fl, fr = dev.fermi_left(energies), dev.fermi_right(energies)
+    obc_sys = OBCSystem(SanchoRubio(convergence_tol=1e-12, per_energy=True), memoization_mode="off")
+    solver = RGF(max_batch_size=B)
+
+    def step():
+        ob = OBCBlocks(n)
+        a00, a01, a10 = A.blocks[0, 0], A.blocks[0, 1], A.blocks[1, 0]
+        g, *_ = obc_sys((a00, a01, a10), contact="left")
+        ob.retarded[0], ob.lesser[0], ob.greater[0] = contact_self_energy(a01, a10, g, fl)
+        ann, an1, a1n = A.blocks[n - 1, n - 1], A.blocks[n - 1, n - 2], A.blocks[n - 2, n - 1]
+        g, *_ = obc_sys((ann, an1, a1n), contact="right")
+        ob.retarded[-1], ob.lesser[-1], ob.greater[-1] = contact_self_energy(an1, a1n, g, fr)
+        cur = solver.selected_solve(A, SL, SG, obc_blocks=ob, out=(XL, XG, XR), return_retarded=True,
+                                    return_current=True)
+        dens = observables.density(XL)
+        return cur, dens
+
+    step()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        cur, dens = step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    elem = 16
+    h2d = 3 * B * proto.nnz * elem + 6 * B * b * b * elem  # A, Sigma^<, Sigma^> + contact blocks
+    d2h = 3 * B * proto.nnz * elem + B * (n + 1) * elem + 6 * B * b * b * elem
+    return {"value": steps * B / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "path": "RGF.selected_solve + OBCSystem(SanchoRubio) + contact_self_energy on pinned host DSDBCOO "
+                    f"stacks, {B} energies per step, {steps} steps"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from quatrex_b200 import EnergyPointSolver, _native, synthetic
+    from quatrex_b200.utils import get_section_sizes
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+    dev = synthetic.cfg1(args.energies)
+    sizes, _ = get_section_sizes(args.energies, world)
+    offs = np.concatenate(([0], np.cumsum(sizes)))
+    mine = np.arange(offs[rank], offs[rank + 1])
+    B = min(args.batch, mine.size)
+    batches = [mine[i:i + B] for i in range(0, mine.size - B + 1, B)] or [mine]
+    fl_all, fr_all = dev.fermi_left(), dev.fermi_right()
+    solver = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True,
+                               device=device)
+    lib = _native.load()
+
+    def step(k):
+        idx = batches[k % len(batches)]
+        return solver.solve(dev.energies[idx], fl_all[idx], fr_all[idx])
+
+    peak = measured_fp64_peak(torch, device)
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(device)
+    gpu_id = str(getattr(props, "uuid", local))
+    if gpu_id and not gpu_id.startswith("GPU-") and len(gpu_id) > 8:
+        gpu_id = "GPU-" + gpu_id
+    clocks = ClockSampler(gpu_id)
+    lib.qtx_profile_reset()
+    lib.qtx_profile_enable(1)
+    sr_iters = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for k in range(args.steps):
+        r = step(args.warmup + k)
+        sr_iters.append(r.sr_iterations)
+    t_end.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    lib.qtx_profile_enable(0)
+    ms = t_start.elapsed_time(t_end)
+    gemm_ms, gemm_flops, gemm_n = _native.profile_read(0)
+    inv_ms, inv_flops, inv_n = _native.profile_read(1)
+    all_ms, _, all_n = _native.profile_read(-1)
+    lib.qtx_profile_reset()
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    done = sum(batches[(args.warmup + k) % len(batches)].size for k in range(args.steps))
+    total = torch.tensor([done], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(total)
+    value = float(total.item()) / (ms_max * 1e-3)
+
+    e2e = None
+    cpu = None
+    if rank == 0 and world == 1:
+        if not args.no_e2e:
+            e2e = e2e_leg(torch, device, dev, dev.energies[np.linspace(0, args.energies - 1, args.e2e_batch)
+                                                               .astype(int)], args.e2e_steps)
+        if not args.no_cpu:
+            cpu = cpu_baseline(args.cpu_energies)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    achieved = (gemm_flops / gemm_n) / ((gemm_ms / gemm_n) * 1e-3) / 1e12 if gemm_n else None
+    roofline = {"bound": "tensor", "kernel": "zgemm (batched complex128 DMMA)", "achieved": achieved,
+                "peak": peak["peak"], "unit": "TFLOP/s",
+                "frac": (achieved / peak["peak"]) if achieved else None,
+                "peak_source": "measured cuBLAS FP64 (max of DGEMM 8192^3, ZGEMM 4096^3) on this GPU; "
+                               "no FP64 entry in MEASURED_PEAKS.json",
+                "peak_detail": peak, "traffic": _ncu_traffic(), "launches": gemm_n,
+                "avg_launch_ms": gemm_ms / gemm_n if gemm_n else None,
+                "share_of_step_time": gemm_ms / ms if ms else None,
+                "zinv_ms_share": inv_ms / ms if ms else None}
+    from quatrex_b200.negf import flops_per_energy
+
+    its = np.mean(np.array(sr_iters), axis=0) if sr_iters else (0, 0)
+    fl = flops_per_energy(32, 256, tuple(float(x) for x in its))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "batch": B, "energies": args.energies,
+                   "parallelism": f"energy sharding x{world}", "l2": "inputs exceed L2 (resident batch state "
+                   f"~{B * 0.45:.0f} GB)", "sr_iterations_mean": [float(x) for x in its]},
+        "roofline": roofline,
+        "as_written_tflops": value * fl["total"] / 1e12,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": all_n,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _ncu_traffic():
+    f = ROOT / "profiles" / "zgemm_traffic.txt"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.startswith("bytes_per_launch_full_batch:"):
+            try:
+                return float(ln.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,229 @@
+/*
+ * qtx_b200.h -- C ABI of the B200 (sm_100a) NEGF hot-path library
+ * (libqtx_b200.so).
+ *
+ * The library replaces the per-energy hot path of the quatrex/qttools
+ * Python package: the block-tridiagonal RGF selected inversion and
+ * selected solve, the Sancho-Rubio open-boundary surface Green's function,
+ * and the transmission / density reductions. The reference has no foreign
+ * function interface of its own (it is NumPy/CuPy Python); each entry point
+ * below names the Python routine whose work it performs, and a ctypes
+ * binding (quatrex_b200/_native.py) calls it from a GFSolver / OBCSolver
+ * subclass with the same Python signature as the reference.
+ *
+ * Conventions
+ *  - Complex numbers are interleaved (re, im): complex128 = 2 x double,
+ *    complex64 = 2 x float (numpy / CuPy / torch layout).
+ *  - Every matrix argument is a strided stack of dense row-major matrices in
+ *    device memory (qtx_mat): element (b, r, c) lives at
+ *    ptr + b * stride + r * ld + c (in complex elements). A qtx_mat with a
+ *    NULL ptr is an all-zero input block, or an output that is not written.
+ *  - A block-tridiagonal stack (qtx_bt) lists its diagonal blocks (i, i),
+ *    upper blocks (i, i+1) and lower blocks (i+1, i) in HOST arrays of
+ *    qtx_mat; block sizes are a host array.
+ *  - All work is enqueued on the given CUDA stream; no call synchronises the
+ *    host unless stated. Calls return QTX_OK (0) or a negative error code;
+ *    qtx_last_error() describes the last failure of the calling thread.
+ *  - Scratch memory is supplied by the caller (workspace pointer + size);
+ *    the *_workspace_size functions give the required size in bytes.
+ *  - Calls on different streams with disjoint buffers and workspaces are
+ *    independent; the library keeps no global mutable state besides the
+ *    thread-local error string.
+ */
+#ifndef QTX_B200_H
+#define QTX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* qtx_stream; /* == cudaStream_t */
+
+enum qtx_status {
+  QTX_OK = 0,
+  QTX_ERR_ARG = -1,       /* invalid argument / shape */
+  QTX_ERR_CUDA = -2,      /* CUDA runtime error */
+  QTX_ERR_WORKSPACE = -3, /* workspace too small */
+  QTX_ERR_SINGULAR = -4,  /* a block had a zero pivot (see info arrays) */
+  QTX_ERR_UNSUPPORTED = -5
+};
+
+enum qtx_dtype { QTX_C128 = 0, QTX_C64 = 1 };
+
+/* Precision of the arithmetic. QTX_FP64: complex128 throughout (FP64
+ * tensor-core MMA). QTX_MIXED: complex64 storage, tensor-core products in
+ * split-BF16 with FP32 accumulation, Newton-Schulz-refined inverses; FP64
+ * only for the pivoted LU of the Schur-complement blocks and for the
+ * Sancho-Rubio convergence test. */
+enum qtx_precision { QTX_FP64 = 0, QTX_MIXED = 1 };
+
+typedef struct qtx_mat {
+  void* ptr;      /* device pointer to element (0, 0) of stack entry 0 */
+  int64_t ld;     /* row stride, complex elements */
+  int64_t stride; /* stack stride, complex elements */
+} qtx_mat;
+
+typedef struct qtx_bt {
+  int32_t num_blocks;
+  const int32_t* block_sizes; /* host, num_blocks entries */
+  const qtx_mat* diag;        /* host, num_blocks entries: block (i, i) */
+  const qtx_mat* upper;       /* host, num_blocks-1 entries: block (i, i+1) */
+  const qtx_mat* lower;       /* host, num_blocks-1 entries: block (i+1, i) */
+} qtx_bt;
+
+/* Flags of qtx_selected_solve. */
+#define QTX_SOLVE_SYMMETRIC_OUT 1 /* X^<, X^> lower blocks are not written
+                                     (qttools out.symmetry, rgf.py:358-359) */
+
+/* Library version, e.g. 100 for 0.1.0. */
+int qtx_version(void);
+
+/* Message describing the last error returned on this thread. */
+const char* qtx_last_error(void);
+
+/* Batched complex128 GEMM, C = alpha op(A) op(B) + beta op(D)
+ * (op: 0 = none, 1 = conjugate transpose; D may be NULL). Building block
+ * of every `@` of qttools/greens_function_solver/rgf.py:71-110,234-428
+ * and boundary_conditions/obc/sancho_rubio.py:64-71. */
+int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                      qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re, double beta_im,
+                      qtx_mat d, int op_d, qtx_mat c, qtx_stream stream);
+
+/* Batched complex128 inverse X = A^{-1} (Gauss-Jordan, partial pivoting).
+ * Replaces qttools/kernels/linalg/inv.py:6-40 (numpy.linalg.inv /
+ * cupy.linalg.solve(a, I)). info: device int[batch], 0 or the 1-based
+ * column of a zero pivot (may be NULL). X may equal A. */
+int qtx_zinv_batched(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, qtx_stream stream);
+
+/* Workspace bytes for qtx_selected_inv on this block layout and batch. */
+size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch);
+
+/* RGF selected inversion: diagonal and first off-diagonal blocks of
+ * (A - OBC)^{-1}, qttools/greens_function_solver/rgf.py:25-113
+ * (RGF.selected_inv). obc_retarded: host array of num_blocks qtx_mat
+ * (NULL ptr = no boundary block on that layer), subtracted from A_ii
+ * (rgf.py:71-74,83-88). x: output blocks; a NULL output block is skipped.
+ * info: device int[batch] singular-pivot report (may be NULL). */
+int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x, int64_t batch,
+                     int* info, void* workspace, size_t workspace_bytes, qtx_stream stream);
+
+/* Workspace bytes for qtx_selected_solve. */
+size_t qtx_selected_solve_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch,
+                                    int return_current);
+
+/* RGF selected solve, qttools/greens_function_solver/rgf.py:115-438
+ * (RGF.selected_solve): X^R = (A - OBC^R)^{-1} (diagonal blocks only, as in
+ * the reference), X^{<,>} = X^R (Sigma^{<,>} + OBC^{<,>}) X^R^H on the
+ * diagonal (anti-Hermitian part, rgf.py:305-310,362-364) and first
+ * off-diagonal blocks. Only the diagonal and upper blocks of sigma_lesser /
+ * sigma_greater are read (rgf.py:222-232,278,291,327-328).
+ *  obc_*: host arrays of num_blocks qtx_mat (NULL ptr = none).
+ *  xr: may be NULL (return_retarded=False).
+ *  current: device complex128 [batch, num_blocks + 1] Meir-Wingreen layer
+ *    current (rgf.py:174-181,388-428), or NULL.
+ *  g0n: optional output of the corner block G^R_{0,N-1} (NULL ptr = skip),
+ *    used for the Caroli transmission.
+ *  density: optional device double [batch, sum(block_sizes)] receiving
+ *    Im diag X^< (quatrex/core/observables.py:8-31), or NULL. */
+int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt* sigma_greater,
+                       const qtx_mat* obc_retarded, const qtx_mat* obc_lesser,
+                       const qtx_mat* obc_greater, const qtx_bt* xl, const qtx_bt* xg,
+                       const qtx_bt* xr, void* current, qtx_mat g0n, double* density,
+                       int flags, int64_t batch, int* info, void* workspace,
+                       size_t workspace_bytes, qtx_stream stream);
+
+/* Workspace bytes for qtx_sancho_rubio. */
+size_t qtx_sancho_rubio_workspace(int n, int64_t batch);
+
+/* Sancho-Rubio surface Green's function,
+ * qttools/boundary_conditions/obc/sancho_rubio.py:33-85 (SanchoRubio.__call__).
+ * x = inv(eps_s) after at most max_iterations decimation steps.
+ *  per_energy = 0: batch-wide stop when max_b delta_b < tol
+ *    (sancho_rubio.py:73-78, the reference semantics);
+ *  per_energy = 1: entries stop individually once delta_b < tol.
+ *  iterations: host int, iterations performed (batch-wide count).
+ *  converged: host int, 1 if the stop criterion was met.
+ *  delta_out: optional device double[batch], final delta per entry.
+ * Synchronises the stream once per iteration to test convergence. */
+int qtx_sancho_rubio(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a_ji, qtx_mat x,
+                     int max_iterations, double tol, int per_energy, int* iterations,
+                     int* converged, double* delta_out, int* info, void* workspace,
+                     size_t workspace_bytes, qtx_stream stream);
+
+/* Workspace bytes sufficient for qtx_contact_self_energy, qtx_obc_refine
+ * and qtx_transmission (square n x n blocks) on `batch` entries. */
+size_t qtx_obc_workspace(int n, int64_t batch);
+
+/* Boundary self-energies of one contact from its surface Green's function
+ * (quatrex/electron/solver.py:483-489):
+ *   sigma   = a_ji g a_ij
+ *   lesser  = i f Gamma,  greater = i (f - 1) Gamma,  Gamma = i (sigma - sigma^H)
+ * occupancies: device double[batch]. Any output may have a NULL ptr. */
+int qtx_contact_self_energy(int n, int64_t batch, qtx_mat a_ij, qtx_mat a_ji, qtx_mat g,
+                            const double* occupancies, qtx_mat sigma, qtx_mat sigma_lesser,
+                            qtx_mat sigma_greater, void* workspace, size_t workspace_bytes,
+                            qtx_stream stream);
+
+/* One fixed-point refinement step with residuals
+ * (qttools/boundary_conditions/obc/obc.py:105-130,156-195):
+ *   x_ref = inv(a_ii - a_ji x a_ij), abs_res = ||x_ref - x||_F,
+ *   rel_res = abs_res / ||x_ref||_F.  x_ref may equal x. */
+int qtx_obc_refine(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a_ji, qtx_mat x,
+                   qtx_mat x_ref, double* rel_res, double* abs_res, int* info, void* workspace,
+                   size_t workspace_bytes, qtx_stream stream);
+
+/* Caroli transmission T = Tr[Gamma_L G_{0,N-1} Gamma_R G_{0,N-1}^H] with
+ * Gamma = i (Sigma - Sigma^H); g0n is m x n (m = first, n = last block
+ * size). The reference computes the same quantity as the boundary
+ * Meir-Wingreen current (rgf.py:414-428) divided by (f_L - f_R) in the
+ * ballistic case. transmission: device double[batch]. */
+int qtx_transmission(int m, int n, int64_t batch, qtx_mat g0n, qtx_mat sigma_left,
+                     qtx_mat sigma_right, double* transmission, void* workspace,
+                     size_t workspace_bytes, qtx_stream stream);
+
+/* DSDBCOO block densification (qttools datastructures/dsdbcoo.py:333-412,
+ * kernels/datastructure/numba/dsdbcoo.py densify_block): the m x n output
+ * blocks are zeroed, then out[b, rows[k], cols[k]] = data[b * data_stride + k]
+ * for k < nnz. data points at the block's first nonzero (block-sorted
+ * storage, dsdbcoo.py:297-331); rows/cols are device int32, block-local. */
+int qtx_coo_densify(int64_t batch, const void* data, int64_t data_stride, int64_t nnz,
+                    const int32_t* rows, const int32_t* cols, qtx_mat out, int m, int n,
+                    qtx_stream stream);
+
+/* Block sparsification (dsdbcoo.py:466-521, sparsify_block):
+ * data[b * data_stride + k] = in[b, rows[k], cols[k]]. */
+int qtx_coo_sparsify(int64_t batch, qtx_mat in, int64_t nnz, const int32_t* rows,
+                     const int32_t* cols, void* data, int64_t data_stride, qtx_stream stream);
+
+/* Diagonal blocks of the system matrix, out[b] = z[b] I - h[b]
+ * (the assembly of quatrex/electron/solver.py:668-709 with zero potential
+ * and scattering self-energy: A(E) = (E + i eta) I - H). h may have stride
+ * 0 (one Hamiltonian block for every energy); z: device complex128[batch]. */
+int qtx_assemble_diag(int n, int64_t batch, qtx_mat h, const void* z, qtx_mat out,
+                      qtx_stream stream);
+
+/* Launch profiler. Kernel classes: */
+enum qtx_kernel_class {
+  QTX_KERNEL_ZGEMM = 0,    /* batched complex GEMM; work = 8 m n k flops */
+  QTX_KERNEL_ZINV = 1,     /* batched inverse; work = 8 n^3 flops */
+  QTX_KERNEL_BLOCKOPS = 2, /* elementwise block kernels; work = bytes */
+  QTX_KERNEL_REDUCE = 3,   /* traces / norms; work = bytes */
+  QTX_KERNEL_FORMAT = 4    /* assembly, densify / sparsify; work = bytes */
+};
+/* Turns event bracketing of every library kernel launch on or off. */
+int qtx_profile_enable(int on);
+/* Drops the recorded launches. */
+int qtx_profile_reset(void);
+/* Sums the recorded launches of one class (kind < 0: all classes):
+ * device milliseconds, algorithmic work and launch count. Synchronizes
+ * the recorded events. */
+int qtx_profile_read(int kind, double* total_ms, double* total_work, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QTX_B200_H */

@@ -1,0 +1,302 @@
+// Memory-bound block kernels of the NEGF path: elementwise combinations
+// with conjugate transposes, the anti-Hermitian projection of X^<, X^> with
+// the density epilogue, traces of products (Meir-Wingreen current), and the
+// per-energy norms of the Sancho-Rubio convergence test and OBC residuals.
+//
+// Transposed operands are staged through a 32x32 shared-memory tile (one
+// padding column) so global loads and stores stay coalesced. Reductions use
+// warp shuffles and one shared-memory combine per CTA; one CTA reduces one
+// stack entry, so results are deterministic.
+#include "common.cuh"
+
+namespace qtx {
+namespace {
+
+constexpr int TILE = 32;
+constexpr int ROWS = 8;  // threads per tile column: block = 32 x 8
+
+struct CombineArgs {
+  MatRef out;
+  Addend t[kMaxAddends];
+  int nterms;
+  int m, n;
+  int64_t batch;
+  const int* active;
+};
+
+// out = sum_t coef_t op_t(X_t) on 32x32 tiles; grid (tiles_n, tiles_m, batch).
+__global__ void __launch_bounds__(TILE* ROWS) zcombine_kernel(const CombineArgs a) {
+  __shared__ z64 tile[TILE][TILE + 1];
+  const int c0 = blockIdx.x * TILE, r0 = blockIdx.y * TILE;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int64_t b = blockIdx.z; b < a.batch; b += gridDim.z) {
+    if (a.active != nullptr && a.active[b] == 0) continue;
+    z64 acc[TILE / ROWS];
+#pragma unroll
+    for (int i = 0; i < TILE / ROWS; ++i) acc[i] = make_double2(0.0, 0.0);
+    for (int t = 0; t < a.nterms; ++t) {
+      const Addend& ad = a.t[t];
+      const z64* p = at<const z64>(ad.m, b);
+      if (!ad.conj_trans) {
+#pragma unroll
+        for (int i = 0; i < TILE / ROWS; ++i) {
+          const int r = r0 + ty + i * ROWS, c = c0 + tx;
+          if (r < a.m && c < a.n) acc[i] = zfma(ad.coef, p[(int64_t)r * ad.m.ld + c], acc[i]);
+        }
+      } else {
+        // op(X)[r][c] = conj(X[c][r]): load the (c0, r0) tile of X coalesced.
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < TILE / ROWS; ++i) {
+          const int xr = c0 + ty + i * ROWS, xc = r0 + tx;  // X row = out col
+          tile[ty + i * ROWS][tx] =
+              (xr < a.n && xc < a.m) ? p[(int64_t)xr * ad.m.ld + xc] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < TILE / ROWS; ++i) {
+          const int r = r0 + ty + i * ROWS, c = c0 + tx;
+          if (r < a.m && c < a.n) acc[i] = zfma(ad.coef, zconj(tile[tx][ty + i * ROWS]), acc[i]);
+        }
+      }
+    }
+    z64* o = at<z64>(a.out, b);
+#pragma unroll
+    for (int i = 0; i < TILE / ROWS; ++i) {
+      const int r = r0 + ty + i * ROWS, c = c0 + tx;
+      if (r < a.m && c < a.n) o[(int64_t)r * a.out.ld + c] = acc[i];
+    }
+  }
+}
+
+// out = 0.5 (X - X^H); density[b * ds + off + r] = Im X[r][r].
+__global__ void __launch_bounds__(TILE* ROWS)
+    zantiherm_kernel(int n, int64_t batch, MatRef X, MatRef out, double* dens, int64_t ds,
+                     int64_t doff) {
+  __shared__ z64 tile[TILE][TILE + 1];
+  const int c0 = blockIdx.x * TILE, r0 = blockIdx.y * TILE;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int64_t b = blockIdx.z; b < batch; b += gridDim.z) {
+    const z64* x = at<const z64>(X, b);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < TILE / ROWS; ++i) {
+      const int xr = c0 + ty + i * ROWS, xc = r0 + tx;
+      tile[ty + i * ROWS][tx] = (xr < n && xc < n) ? x[(int64_t)xr * X.ld + xc] : make_double2(0, 0);
+    }
+    __syncthreads();
+    z64* o = out.null() ? nullptr : at<z64>(out, b);
+#pragma unroll
+    for (int i = 0; i < TILE / ROWS; ++i) {
+      const int r = r0 + ty + i * ROWS, c = c0 + tx;
+      if (r < n && c < n) {
+        const z64 v = x[(int64_t)r * X.ld + c];
+        const z64 w = tile[tx][ty + i * ROWS];  // X[c][r]
+        const z64 h = make_double2(0.5 * (v.x - w.x), 0.5 * (v.y + w.y));
+        if (o != nullptr) o[(int64_t)r * out.ld + c] = h;
+        if (dens != nullptr && r == c) dens[b * ds + doff + r] = h.y;
+      }
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  T s = 0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w) s += red[w];
+  return s;
+}
+
+// One CTA per stack entry: Tr(X Y) = sum_{r,c} X[r][c] Y[c][r], via 32x32
+// tiles (Y tile staged transposed).
+__global__ void __launch_bounds__(256) ztrace_kernel(int n, int64_t batch, MatRef X, MatRef Y,
+                                                     z64 coef, z64* res, int64_t rs, int64_t roff,
+                                                     int accumulate) {
+  __shared__ z64 tile[TILE][TILE + 1];
+  __shared__ double red[8];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const z64* x = at<const z64>(X, b);
+    const z64* y = at<const z64>(Y, b);
+    double sre = 0.0, sim = 0.0;
+    for (int r0 = 0; r0 < n; r0 += TILE)
+      for (int c0 = 0; c0 < n; c0 += TILE) {
+        __syncthreads();
+        // tile <- Y[c0.., r0..]
+#pragma unroll
+        for (int i = 0; i < TILE / ROWS; ++i) {
+          const int yr = c0 + ty + i * ROWS, yc = r0 + tx;
+          tile[ty + i * ROWS][tx] = (yr < n && yc < n) ? y[(int64_t)yr * Y.ld + yc] : make_double2(0, 0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < TILE / ROWS; ++i) {
+          const int r = r0 + ty + i * ROWS, c = c0 + tx;
+          if (r < n && c < n) {
+            const z64 a = x[(int64_t)r * X.ld + c];
+            const z64 w = tile[tx][ty + i * ROWS];  // Y[c][r]
+            sre += a.x * w.x - a.y * w.y;
+            sim += a.x * w.y + a.y * w.x;
+          }
+        }
+      }
+    sre = block_sum(sre, red);
+    sim = block_sum(sim, red);
+    if (threadIdx.x == 0) {
+      const z64 v = zmul(coef, make_double2(sre, sim));
+      z64* o = res + b * rs + roff;
+      *o = accumulate ? zadd(*o, v) : v;
+    }
+  }
+}
+
+// delta[b] = sqrt(sum (|x| + |y|)^2) / 2.
+__global__ void __launch_bounds__(256) sr_delta_kernel(int n, int64_t batch, MatRef X, MatRef Y,
+                                                       double* delta, const int* active) {
+  __shared__ double red[8];
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    if (active != nullptr && active[b] == 0) continue;
+    const z64* x = at<const z64>(X, b);
+    const z64* y = at<const z64>(Y, b);
+    double s = 0.0;
+    for (int64_t idx = threadIdx.x; idx < (int64_t)n * n; idx += blockDim.x) {
+      const int r = (int)(idx / n), c = (int)(idx % n);
+      const z64 a = x[(int64_t)r * X.ld + c];
+      const z64 w = y[(int64_t)r * Y.ld + c];
+      const double v = hypot(a.x, a.y) + hypot(w.x, w.y);
+      s += v * v;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) delta[b] = 0.5 * sqrt(s);
+  }
+}
+
+__global__ void __launch_bounds__(256) znorm_diff_kernel(int n, int64_t batch, MatRef X, MatRef Y,
+                                                         double* nd, double* nx, double* rel) {
+  __shared__ double red[8];
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const z64* x = at<const z64>(X, b);
+    const z64* y = at<const z64>(Y, b);
+    double sd = 0.0, sx = 0.0;
+    for (int64_t idx = threadIdx.x; idx < (int64_t)n * n; idx += blockDim.x) {
+      const int r = (int)(idx / n), c = (int)(idx % n);
+      const z64 a = x[(int64_t)r * X.ld + c];
+      const z64 w = y[(int64_t)r * Y.ld + c];
+      const double dr = a.x - w.x, di = a.y - w.y;
+      sd += dr * dr + di * di;
+      sx += a.x * a.x + a.y * a.y;
+    }
+    sd = block_sum(sd, red);
+    sx = block_sum(sx, red);
+    if (threadIdx.x == 0) {
+      if (nd != nullptr) nd[b] = sqrt(sd);
+      if (nx != nullptr) nx[b] = sqrt(sx);
+      if (rel != nullptr) rel[b] = sqrt(sd) / sqrt(sx);
+    }
+  }
+}
+
+// out[b] = Re sum conj(G) .* P  (= Re Tr(P G^H)).
+__global__ void __launch_bounds__(256) zre_inner_kernel(int m, int n, int64_t batch, MatRef P,
+                                                        MatRef G, double* out) {
+  __shared__ double red[8];
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const z64* p = at<const z64>(P, b);
+    const z64* g = at<const z64>(G, b);
+    double s = 0.0;
+    for (int64_t idx = threadIdx.x; idx < (int64_t)m * n; idx += blockDim.x) {
+      const int r = (int)(idx / n), c = (int)(idx % n);
+      const z64 a = p[(int64_t)r * P.ld + c];
+      const z64 w = g[(int64_t)r * G.ld + c];
+      s += a.x * w.x + a.y * w.y;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[b] = s;
+  }
+}
+
+unsigned grid_z(int64_t batch) { return (unsigned)(batch < 65535 ? batch : 65535); }
+unsigned grid_x(int64_t batch) { return (unsigned)(batch < 1048576 ? batch : 1048576); }
+
+}  // namespace
+
+int zcombine(int m, int n, int64_t batch, MatRef out, const Addend* terms, int nterms,
+             const int* active, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || batch <= 0) return QTX_OK;
+  CombineArgs a{};
+  a.out = out;
+  a.m = m;
+  a.n = n;
+  a.batch = batch;
+  a.active = active;
+  a.nterms = 0;
+  for (int t = 0; t < nterms; ++t) {
+    if (terms[t].m.null()) continue;
+    if (a.nterms >= kMaxAddends) {
+      set_error("zcombine: too many terms");
+      return QTX_ERR_ARG;
+    }
+    a.t[a.nterms++] = terms[t];
+  }
+  dim3 grid((n + TILE - 1) / TILE, (m + TILE - 1) / TILE, grid_z(batch));
+  ProfScope prof(QTX_KERNEL_BLOCKOPS, 16.0 * m * n * (double)batch * (a.nterms + 1), s);
+  zcombine_kernel<<<grid, dim3(TILE, ROWS), 0, s>>>(a);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+int zantiherm(int n, int64_t batch, MatRef X, MatRef out, double* density, int64_t dens_stride,
+              int64_t dens_off, cudaStream_t s) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  dim3 grid((n + TILE - 1) / TILE, (n + TILE - 1) / TILE, grid_z(batch));
+  ProfScope prof(QTX_KERNEL_BLOCKOPS, 32.0 * n * n * (double)batch, s);
+  zantiherm_kernel<<<grid, dim3(TILE, ROWS), 0, s>>>(n, batch, X, out, density, dens_stride,
+                                                     dens_off);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+int ztrace_prod(int n, int64_t batch, MatRef X, MatRef Y, z64 coef, z64* result, int64_t rstride,
+                int64_t roff, int accumulate, cudaStream_t s) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  ProfScope prof(QTX_KERNEL_REDUCE, 32.0 * n * n * (double)batch, s);
+  ztrace_kernel<<<grid_x(batch), 256, 0, s>>>(n, batch, X, Y, coef, result, rstride, roff,
+                                              accumulate);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+int sr_delta(int n, int64_t batch, MatRef X, MatRef Y, double* delta, const int* active,
+             cudaStream_t s) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  ProfScope prof(QTX_KERNEL_REDUCE, 32.0 * n * n * (double)batch, s);
+  sr_delta_kernel<<<grid_x(batch), 256, 0, s>>>(n, batch, X, Y, delta, active);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+int znorm_diff(int n, int64_t batch, MatRef X, MatRef Y, double* nrm_diff, double* nrm,
+               double* rel, cudaStream_t s) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  ProfScope prof(QTX_KERNEL_REDUCE, 32.0 * n * n * (double)batch, s);
+  znorm_diff_kernel<<<grid_x(batch), 256, 0, s>>>(n, batch, X, Y, nrm_diff, nrm, rel);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+int zre_inner(int m, int n, int64_t batch, MatRef P, MatRef G, double* out, cudaStream_t s) {
+  if (m <= 0 || n <= 0 || batch <= 0) return QTX_OK;
+  ProfScope prof(QTX_KERNEL_REDUCE, 32.0 * m * n * (double)batch, s);
+  zre_inner_kernel<<<grid_x(batch), 256, 0, s>>>(m, n, batch, P, G, out);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+}  // namespace qtx

@@ -1,0 +1,340 @@
+// extern "C" entry points of libqtx_b200.so (declared in include/qtx_b200.h).
+//
+// Each wrapper validates its arguments, zeroes the caller's status arrays,
+// binds the caller's workspace and forwards to the drivers in rgf.cu /
+// sr.cu. No C++ exception crosses the ABI; failures return a negative
+// qtx_status and leave a message for qtx_last_error().
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "common.cuh"
+
+namespace qtx {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void set_error(const std::string& msg) { g_error = msg; }
+const char* get_error() { return g_error.c_str(); }
+
+// Drivers (rgf.cu, sr.cu).
+int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_t batch, int* info,
+                     Workspace& ws, cudaStream_t s);
+int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaStream_t s);
+size_t sancho_rubio_ws(int n, int64_t batch);
+int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
+                     int max_iterations, double tol, int per_energy, int* iterations,
+                     int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s);
+size_t obc_refine_ws(int n, int64_t batch);
+int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x, MatRef xref,
+                   double* rel, double* abs_res, int* info, Workspace& ws, cudaStream_t s);
+size_t contact_ws(int n, int64_t batch);
+int contact_run(int n, int64_t batch, MatRef aij, MatRef aji, MatRef g, const double* occ,
+                MatRef sigma, MatRef sl, MatRef sg, Workspace& ws, cudaStream_t s);
+size_t transmission_ws(int m, int n, int64_t batch);
+int transmission_run(int m, int n, int64_t batch, MatRef g0n, MatRef sl, MatRef sr, double* T,
+                     Workspace& ws, cudaStream_t s);
+
+}  // namespace qtx
+
+using namespace qtx;
+
+namespace {
+
+int check_bt(const qtx_bt* t, const char* name, int n_expected, const int32_t* bs_expected) {
+  if (t == nullptr) return QTX_OK;
+  if (t->num_blocks <= 0 || t->block_sizes == nullptr) {
+    set_error(std::string(name) + ": invalid block layout");
+    return QTX_ERR_ARG;
+  }
+  if (n_expected > 0) {
+    if (t->num_blocks != n_expected) {
+      set_error(std::string(name) + ": number of blocks differs from the system matrix");
+      return QTX_ERR_ARG;
+    }
+    for (int i = 0; i < n_expected; ++i)
+      if (t->block_sizes[i] != bs_expected[i]) {
+        set_error(std::string(name) + ": block sizes differ from the system matrix");
+        return QTX_ERR_ARG;
+      }
+  }
+  for (int i = 0; i < t->num_blocks; ++i)
+    if (t->block_sizes[i] <= 0 || t->block_sizes[i] > 1024) {
+      set_error(std::string(name) + ": block sizes must be in [1, 1024]");
+      return QTX_ERR_ARG;
+    }
+  return QTX_OK;
+}
+
+std::vector<MatRef> obc_vec(const qtx_mat* o, int n) {
+  std::vector<MatRef> v;
+  if (o == nullptr) return v;
+  v.resize(n);
+  for (int i = 0; i < n; ++i) v[i] = from_abi(o[i]);
+  return v;
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    set_error(std::string("internal error: ") + e.what());
+    return QTX_ERR_ARG;
+  } catch (...) {
+    set_error("internal error");
+    return QTX_ERR_ARG;
+  }
+}
+
+Workspace bind(void* base, size_t bytes) {
+  Workspace ws;
+  ws.base = static_cast<char*>(base);
+  ws.cap = bytes;
+  return ws;
+}
+
+int need_ws(void* base, size_t bytes, size_t need, const char* who) {
+  if (need > 0 && (base == nullptr || bytes < need)) {
+    set_error(std::string(who) + ": workspace too small (" + std::to_string(bytes) + " < " +
+              std::to_string(need) + " bytes)");
+    return QTX_ERR_WORKSPACE;
+  }
+  return QTX_OK;
+}
+
+size_t solve_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch, int cur) {
+  // Mirrors the allocation order of selected_solve_run.
+  Workspace ws;
+  int bm = 0;
+  for (int i = 0; i < nb; ++i) bm = bs[i] > bm ? bs[i] : bm;
+  const int sets = 3 + (cur ? 2 : 0);
+  for (int k = 0; k < sets; ++k)
+    for (int i = 0; i < nb; ++i) ws.mat(bs[i], bs[i], batch);
+  for (int k = 0; k < 19; ++k) ws.mat(bm, bm, batch);
+  return ws.off + 256;
+}
+
+size_t inv_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch) {
+  Workspace ws;
+  int bm = 0;
+  for (int i = 0; i < nb; ++i) bm = bs[i] > bm ? bs[i] : bm;
+  for (int i = 0; i < nb; ++i) ws.mat(bs[i], bs[i], batch);
+  for (int k = 0; k < 6; ++k) ws.mat(bm, bm, batch);
+  return ws.off + 256;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qtx_version(void) { return 100; }
+
+const char* qtx_last_error(void) { return get_error(); }
+
+int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                      qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re, double beta_im,
+                      qtx_mat d, int op_d, qtx_mat c, qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || k < 0 || batch < 0 || (op_a != 0 && op_a != 1) ||
+        (op_b != 0 && op_b != 1) || (op_d != 0 && op_d != 1)) {
+      set_error("qtx_zgemm_batched: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    if (c.ptr == nullptr) {
+      set_error("qtx_zgemm_batched: null output");
+      return (int)QTX_ERR_ARG;
+    }
+    GemmDesc g;
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.batch = batch;
+    g.A = from_abi(a);
+    g.B = from_abi(b);
+    g.opA = op_a;
+    g.opB = op_b;
+    g.alpha = make_double2(alpha_re, alpha_im);
+    g.C = from_abi(c);
+    if (d.ptr != nullptr) {
+      g.add[0] = Addend{from_abi(d), make_double2(beta_re, beta_im), op_d};
+      g.nadd = 1;
+    }
+    return zgemm(g, (cudaStream_t)stream);
+  });
+}
+
+int qtx_zinv_batched(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, qtx_stream stream) {
+  return guarded([&] {
+    if (n < 0 || batch < 0 || a.ptr == nullptr || x.ptr == nullptr) {
+      set_error("qtx_zinv_batched: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, (cudaStream_t)stream));
+    return zinv(n, batch, from_abi(a), from_abi(x), info, nullptr, (cudaStream_t)stream);
+  });
+}
+
+size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch) {
+  if (num_blocks <= 0 || block_sizes == nullptr || batch <= 0) return 0;
+  return inv_ws_bytes(num_blocks, block_sizes, batch);
+}
+
+int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x, int64_t batch,
+                     int* info, void* workspace, size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (a == nullptr || x == nullptr || batch <= 0) {
+      set_error("qtx_selected_inv: null matrix or empty batch");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(check_bt(a, "a", 0, nullptr));
+    QTX_TRY(check_bt(x, "x", a->num_blocks, a->block_sizes));
+    const size_t need = inv_ws_bytes(a->num_blocks, a->block_sizes, batch);
+    QTX_TRY(need_ws(workspace, workspace_bytes, need, "qtx_selected_inv"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+    BTRef A = bt_from_abi(a), X = bt_from_abi(x);
+    std::vector<MatRef> o = obc_vec(obc_retarded, a->num_blocks);
+    Workspace ws = bind(workspace, workspace_bytes);
+    return selected_inv_run(A, o.empty() ? nullptr : o.data(), X, batch, info, ws, s);
+  });
+}
+
+size_t qtx_selected_solve_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch,
+                                    int return_current) {
+  if (num_blocks <= 0 || block_sizes == nullptr || batch <= 0) return 0;
+  return solve_ws_bytes(num_blocks, block_sizes, batch, return_current);
+}
+
+int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt* sigma_greater,
+                       const qtx_mat* obc_retarded, const qtx_mat* obc_lesser,
+                       const qtx_mat* obc_greater, const qtx_bt* xl, const qtx_bt* xg,
+                       const qtx_bt* xr, void* current, qtx_mat g0n, double* density, int flags,
+                       int64_t batch, int* info, void* workspace, size_t workspace_bytes,
+                       qtx_stream stream) {
+  return guarded([&] {
+    if (a == nullptr || batch <= 0) {
+      set_error("qtx_selected_solve: null system matrix or empty batch");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(check_bt(a, "a", 0, nullptr));
+    const int N = a->num_blocks;
+    QTX_TRY(check_bt(sigma_lesser, "sigma_lesser", N, a->block_sizes));
+    QTX_TRY(check_bt(sigma_greater, "sigma_greater", N, a->block_sizes));
+    QTX_TRY(check_bt(xl, "xl", N, a->block_sizes));
+    QTX_TRY(check_bt(xg, "xg", N, a->block_sizes));
+    QTX_TRY(check_bt(xr, "xr", N, a->block_sizes));
+    const size_t need = solve_ws_bytes(N, a->block_sizes, batch, current != nullptr);
+    QTX_TRY(need_ws(workspace, workspace_bytes, need, "qtx_selected_solve"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+    if (current)
+      QTX_CHECK_CUDA(cudaMemsetAsync(current, 0, sizeof(z64) * batch * (N + 1), s));
+    SolveIO io;
+    io.a = bt_from_abi(a);
+    io.sl = bt_from_abi(sigma_lesser);
+    io.sg = bt_from_abi(sigma_greater);
+    io.xl = bt_from_abi(xl);
+    io.xg = bt_from_abi(xg);
+    io.xr = bt_from_abi(xr);
+    std::vector<MatRef> orr = obc_vec(obc_retarded, N), ol = obc_vec(obc_lesser, N),
+                        og = obc_vec(obc_greater, N);
+    io.obc_r = orr.empty() ? nullptr : orr.data();
+    io.obc_l = ol.empty() ? nullptr : ol.data();
+    io.obc_g = og.empty() ? nullptr : og.data();
+    io.current = static_cast<z64*>(current);
+    io.g0n = from_abi(g0n);
+    io.density = density;
+    io.symmetric = (flags & QTX_SOLVE_SYMMETRIC_OUT) ? 1 : 0;
+    Workspace ws = bind(workspace, workspace_bytes);
+    return selected_solve_run(io, batch, info, ws, s);
+  });
+}
+
+size_t qtx_sancho_rubio_workspace(int n, int64_t batch) {
+  if (n <= 0 || batch <= 0) return 0;
+  return sancho_rubio_ws(n, batch);
+}
+
+int qtx_sancho_rubio(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a_ji, qtx_mat x,
+                     int max_iterations, double tol, int per_energy, int* iterations,
+                     int* converged, double* delta_out, int* info, void* workspace,
+                     size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (n <= 0 || n > 1024 || batch <= 0 || max_iterations < 0 || a_ii.ptr == nullptr ||
+        x.ptr == nullptr) {
+      set_error("qtx_sancho_rubio: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, sancho_rubio_ws(n, batch), "qtx_sancho_rubio"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return sancho_rubio_run(n, batch, from_abi(a_ii), from_abi(a_ij), from_abi(a_ji), from_abi(x),
+                            max_iterations, tol, per_energy, iterations, converged, delta_out, info,
+                            ws, s);
+  });
+}
+
+size_t qtx_obc_workspace(int n, int64_t batch) {
+  if (n <= 0 || batch <= 0) return 0;
+  size_t w = contact_ws(n, batch);
+  const size_t r = obc_refine_ws(n, batch), t = transmission_ws(n, n, batch);
+  if (r > w) w = r;
+  if (t > w) w = t;
+  return w;
+}
+
+int qtx_contact_self_energy(int n, int64_t batch, qtx_mat a_ij, qtx_mat a_ji, qtx_mat g,
+                            const double* occupancies, qtx_mat sigma, qtx_mat sigma_lesser,
+                            qtx_mat sigma_greater, void* workspace, size_t workspace_bytes,
+                            qtx_stream stream) {
+  return guarded([&] {
+    if (n <= 0 || batch <= 0 || g.ptr == nullptr) {
+      set_error("qtx_contact_self_energy: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, contact_ws(n, batch), "qtx_contact_self_energy"));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return contact_run(n, batch, from_abi(a_ij), from_abi(a_ji), from_abi(g), occupancies,
+                       from_abi(sigma), from_abi(sigma_lesser), from_abi(sigma_greater), ws,
+                       (cudaStream_t)stream);
+  });
+}
+
+int qtx_obc_refine(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a_ji, qtx_mat x,
+                   qtx_mat x_ref, double* rel_res, double* abs_res, int* info, void* workspace,
+                   size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (n <= 0 || n > 1024 || batch <= 0 || x.ptr == nullptr || x_ref.ptr == nullptr) {
+      set_error("qtx_obc_refine: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, obc_refine_ws(n, batch), "qtx_obc_refine"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return obc_refine_run(n, batch, from_abi(a_ii), from_abi(a_ij), from_abi(a_ji), from_abi(x),
+                          from_abi(x_ref), rel_res, abs_res, info, ws, s);
+  });
+}
+
+int qtx_transmission(int m, int n, int64_t batch, qtx_mat g0n, qtx_mat sigma_left,
+                     qtx_mat sigma_right, double* transmission, void* workspace,
+                     size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (m <= 0 || n <= 0 || batch <= 0 || g0n.ptr == nullptr || sigma_left.ptr == nullptr ||
+        sigma_right.ptr == nullptr || transmission == nullptr) {
+      set_error("qtx_transmission: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, transmission_ws(m, n, batch), "qtx_transmission"));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return transmission_run(m, n, batch, from_abi(g0n), from_abi(sigma_left),
+                            from_abi(sigma_right), transmission, ws, (cudaStream_t)stream);
+  });
+}
+
+}  // extern "C"

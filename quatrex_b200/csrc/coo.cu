@@ -1,0 +1,135 @@
+// DSDBCOO <-> dense block conversion on the device.
+//
+// qttools stores a DSDBSparse stack as data[stack, nnz] with block-sorted
+// COO indices (datastructures/dsdbcoo.py:297-331, 886-977); reading a block
+// densifies it (dsdbcoo.py:333-412, kernels/datastructure/*/dsdbcoo.py
+// densify_block) and writing sparsifies it (dsdbcoo.py:466-521). Blocks
+// whose nnz equals b_i * b_j in row-major order need neither: the solver
+// reads and writes them in place. The kernels below handle all other
+// blocks: one thread per (stack entry, nonzero), grid-strided.
+#include "common.cuh"
+
+namespace qtx {
+namespace {
+
+__global__ void zero_kernel(MatRef out, int m, int n, int64_t batch) {
+  const int64_t per = (int64_t)m * n;
+  const int64_t total = per * batch;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / per, e = i % per;
+    const int r = (int)(e / n), c = (int)(e % n);
+    at<z64>(out, b)[(int64_t)r * out.ld + c] = make_double2(0.0, 0.0);
+  }
+}
+
+__global__ void densify_kernel(int64_t batch, const z64* data, int64_t dstride, int64_t nnz,
+                               const int32_t* rows, const int32_t* cols, MatRef out, int m, int n) {
+  const int64_t total = nnz * batch;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / nnz, k = i % nnz;
+    const int r = rows[k], c = cols[k];
+    if (r < 0 || r >= m || c < 0 || c >= n) continue;
+    at<z64>(out, b)[(int64_t)r * out.ld + c] = data[b * dstride + k];
+  }
+}
+
+__global__ void sparsify_kernel(int64_t batch, MatRef in, int64_t nnz, const int32_t* rows,
+                                const int32_t* cols, z64* data, int64_t dstride) {
+  const int64_t total = nnz * batch;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / nnz, k = i % nnz;
+    data[b * dstride + k] = at<const z64>(in, b)[(int64_t)rows[k] * in.ld + cols[k]];
+  }
+}
+
+unsigned blocks_for(int64_t total) {
+  const int64_t b = (total + 255) / 256;
+  return (unsigned)(b < 148 * 64 ? (b > 0 ? b : 1) : 148 * 64);
+}
+
+}  // namespace
+}  // namespace qtx
+
+using namespace qtx;
+
+extern "C" int qtx_coo_densify(int64_t batch, const void* data, int64_t data_stride, int64_t nnz,
+                               const int32_t* rows, const int32_t* cols, qtx_mat out, int m, int n,
+                               qtx_stream stream) {
+  if (batch < 0 || nnz < 0 || m < 0 || n < 0 || out.ptr == nullptr ||
+      (nnz > 0 && (data == nullptr || rows == nullptr || cols == nullptr))) {
+    set_error("qtx_coo_densify: invalid arguments");
+    return QTX_ERR_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const MatRef o = from_abi(out);
+  if ((int64_t)m * n * batch > 0) {
+    ProfScope prof(QTX_KERNEL_FORMAT, 16.0 * m * n * (double)batch, s);
+    zero_kernel<<<blocks_for((int64_t)m * n * batch), 256, 0, s>>>(o, m, n, batch);
+    QTX_CHECK_LAUNCH();
+  }
+  if (nnz * batch > 0) {
+    ProfScope prof(QTX_KERNEL_FORMAT, 32.0 * nnz * (double)batch, s);
+    densify_kernel<<<blocks_for(nnz * batch), 256, 0, s>>>(
+        batch, static_cast<const z64*>(data), data_stride, nnz, rows, cols, o, m, n);
+    QTX_CHECK_LAUNCH();
+  }
+  return QTX_OK;
+}
+
+extern "C" int qtx_coo_sparsify(int64_t batch, qtx_mat in, int64_t nnz, const int32_t* rows,
+                                const int32_t* cols, void* data, int64_t data_stride,
+                                qtx_stream stream) {
+  if (batch < 0 || nnz < 0 || in.ptr == nullptr ||
+      (nnz > 0 && (data == nullptr || rows == nullptr || cols == nullptr))) {
+    set_error("qtx_coo_sparsify: invalid arguments");
+    return QTX_ERR_ARG;
+  }
+  if (nnz * batch == 0) return QTX_OK;
+  ProfScope prof(QTX_KERNEL_FORMAT, 32.0 * nnz * (double)batch, (cudaStream_t)stream);
+  sparsify_kernel<<<blocks_for(nnz * batch), 256, 0, (cudaStream_t)stream>>>(
+      batch, from_abi(in), nnz, rows, cols, static_cast<z64*>(data), data_stride);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// System-matrix diagonal blocks A_ii(E) = z I - H_ii (quatrex
+// electron/solver.py:668-709 with zero potential and scattering
+// self-energy). h may have stack stride 0 (one Hamiltonian block shared by
+// every energy).
+// ---------------------------------------------------------------------------
+namespace qtx {
+namespace {
+__global__ void assemble_diag_kernel(int n, int64_t batch, MatRef h, const z64* z, MatRef out) {
+  const int64_t per = (int64_t)n * n;
+  const int64_t total = per * batch;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / per, e = i % per;
+    const int r = (int)(e / n), c = (int)(e % n);
+    const z64 v = at<const z64>(h, b)[(int64_t)r * h.ld + c];
+    z64 o = make_double2(-v.x, -v.y);
+    if (r == c) o = zadd(o, z[b]);
+    at<z64>(out, b)[(int64_t)r * out.ld + c] = o;
+  }
+}
+}  // namespace
+}  // namespace qtx
+
+extern "C" int qtx_assemble_diag(int n, int64_t batch, qtx_mat h, const void* z, qtx_mat out,
+                                 qtx_stream stream) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  if (h.ptr == nullptr || z == nullptr || out.ptr == nullptr) {
+    set_error("qtx_assemble_diag: null argument");
+    return QTX_ERR_ARG;
+  }
+  const int64_t total = (int64_t)n * n * batch;
+  ProfScope prof(QTX_KERNEL_FORMAT, 32.0 * (double)total, (cudaStream_t)stream);
+  assemble_diag_kernel<<<blocks_for(total), 256, 0, (cudaStream_t)stream>>>(
+      n, batch, from_abi(h), static_cast<const z64*>(z), from_abi(out));
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}

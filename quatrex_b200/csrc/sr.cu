@@ -1,0 +1,272 @@
+// Open-boundary conditions: Sancho-Rubio decimation, the OBCSystem
+// fixed-point refinement, contact self-energies and the Caroli
+// transmission.
+//
+// Sancho-Rubio (qttools boundary_conditions/obc/sancho_rubio.py:33-85):
+//   inv = eps^-1;  eps -= alpha inv beta + beta inv alpha;
+//   eps_s -= alpha inv beta;  alpha = alpha inv alpha;  beta = beta inv beta
+// As written that is one inverse and ten products per step; here
+// alpha inv and beta inv are formed once and reused (six products), the
+// eps_s update is the second output of the alpha inv beta product, and the
+// convergence measure ||(|alpha| + |beta|)||_F / 2 is one FP64 reduction
+// per energy. Every loop is bounded by max_iterations.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace qtx {
+
+namespace {
+
+const z64 ONE{1.0, 0.0};
+const z64 MONE{-1.0, 0.0};
+
+__global__ void fill_int_kernel(int* p, int64_t n, int v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// lesser = -f (S - S^H), greater = -(f - 1) (S - S^H)   (i f Gamma with
+// Gamma = i (S - S^H)); 32x32 tiles, S^H staged through shared memory.
+__global__ void __launch_bounds__(256) gamma_scale_kernel(int n, int64_t batch, MatRef S,
+                                                          const double* occ, MatRef L, MatRef G) {
+  __shared__ z64 tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int64_t b = blockIdx.z; b < batch; b += gridDim.z) {
+    const z64* s = at<const z64>(S, b);
+    __syncthreads();
+    for (int i = 0; i < 4; ++i) {
+      const int sr = c0 + ty + i * 8, sc = r0 + tx;
+      tile[ty + i * 8][tx] = (sr < n && sc < n) ? s[(int64_t)sr * S.ld + sc] : make_double2(0, 0);
+    }
+    __syncthreads();
+    const double f = occ[b];
+    for (int i = 0; i < 4; ++i) {
+      const int r = r0 + ty + i * 8, c = c0 + tx;
+      if (r >= n || c >= n) continue;
+      const z64 v = s[(int64_t)r * S.ld + c];
+      const z64 w = tile[tx][ty + i * 8];  // S[c][r]
+      const z64 d = make_double2(v.x - w.x, v.y + w.y);  // S - S^H
+      if (!L.null()) at<z64>(L, b)[(int64_t)r * L.ld + c] = make_double2(-f * d.x, -f * d.y);
+      if (!G.null())
+        at<z64>(G, b)[(int64_t)r * G.ld + c] = make_double2(-(f - 1.0) * d.x, -(f - 1.0) * d.y);
+    }
+  }
+}
+
+int fill_int(int* p, int64_t n, int v, cudaStream_t s) {
+  if (n <= 0) return QTX_OK;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4096);
+  ProfScope prof(QTX_KERNEL_BLOCKOPS, 4.0 * (double)n, s);
+  fill_int_kernel<<<blocks, 256, 0, s>>>(p, n, v);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+struct G {
+  GemmDesc d;
+  G(int M, int N, int K, int64_t batch, MatRef A, MatRef B, MatRef C, z64 alpha = ONE) {
+    d.M = M;
+    d.N = N;
+    d.K = K;
+    d.batch = batch;
+    d.A = A;
+    d.B = B;
+    d.C = C;
+    d.alpha = alpha;
+  }
+  G& plus(const MatRef& m, z64 c, int ct = 0) {
+    if (!m.null()) d.add[d.nadd++] = Addend{m, c, ct};
+    return *this;
+  }
+  G& second(const MatRef& c3, z64 scale) {
+    d.C3 = c3;
+    d.scale3 = scale;
+    return *this;
+  }
+  G& plus3(const MatRef& m, z64 c) {
+    if (!m.null()) d.add[d.nadd + d.nadd3++] = Addend{m, c, 0};
+    return *this;
+  }
+  G& mask(const int* a) {
+    d.active = a;
+    return *this;
+  }
+  int run(cudaStream_t s) { return zgemm(d, s); }
+};
+
+}  // namespace
+
+size_t sancho_rubio_ws(int n, int64_t batch) {
+  Workspace ws;
+  for (int k = 0; k < 10; ++k) ws.mat(n, n, batch);
+  ws.take(sizeof(double) * batch);
+  ws.take(sizeof(int) * batch);
+  return ws.off + 256;
+}
+
+int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
+                     int max_iterations, double tol, int per_energy, int* iterations,
+                     int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s) {
+  MatRef eps = ws.mat(n, n, batch), eps_s = ws.mat(n, n, batch);
+  MatRef alpha[2] = {ws.mat(n, n, batch), ws.mat(n, n, batch)};
+  MatRef beta[2] = {ws.mat(n, n, batch), ws.mat(n, n, batch)};
+  MatRef inv_e = ws.mat(n, n, batch), aI = ws.mat(n, n, batch), bI = ws.mat(n, n, batch);
+  MatRef t1 = ws.mat(n, n, batch);
+  double* delta = static_cast<double*>(ws.take(sizeof(double) * batch));
+  int* active = static_cast<int*>(ws.take(sizeof(int) * batch));
+  if (ws.overflow) {
+    set_error("sancho_rubio: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  {
+    Addend t = Addend{aii, ONE, 0};
+    QTX_TRY(zcombine(n, n, batch, eps, &t, 1, nullptr, s));
+    QTX_TRY(zcombine(n, n, batch, eps_s, &t, 1, nullptr, s));
+    Addend u = Addend{aji, ONE, 0};
+    QTX_TRY(zcombine(n, n, batch, alpha[0], &u, 1, nullptr, s));
+    Addend v = Addend{aij, ONE, 0};
+    QTX_TRY(zcombine(n, n, batch, beta[0], &v, 1, nullptr, s));
+  }
+  QTX_TRY(fill_int(active, batch, 1, s));
+  std::vector<double> hdelta(batch);
+  std::vector<int> hactive(batch, 1);
+  int it = 0, cur = 0;
+  bool done = false;
+  const int* mask = per_energy ? active : nullptr;
+  while (it < max_iterations && !done) {
+    const int nx = cur ^ 1;
+    QTX_TRY(zinv(n, batch, eps, inv_e, info, mask, s));
+    QTX_TRY(G(n, n, n, batch, alpha[cur], inv_e, aI).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, beta[cur], inv_e, bI).mask(mask).run(s));
+    // t1 = alpha inv beta;  eps_s <- eps_s - t1.
+    QTX_TRY(G(n, n, n, batch, aI, beta[cur], t1).second(eps_s, MONE).plus3(eps_s, ONE).mask(mask).run(s));
+    // eps <- eps - t1 - beta inv alpha.
+    QTX_TRY(G(n, n, n, batch, bI, alpha[cur], eps, MONE).plus(eps, ONE).plus(t1, MONE).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, aI, alpha[cur], alpha[nx]).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, bI, beta[cur], beta[nx]).mask(mask).run(s));
+    QTX_TRY(sr_delta(n, batch, alpha[nx], beta[nx], delta, mask, s));
+    ++it;
+    QTX_CHECK_CUDA(cudaMemcpyAsync(hdelta.data(), delta, sizeof(double) * batch,
+                                   cudaMemcpyDeviceToHost, s));
+    QTX_CHECK_CUDA(cudaStreamSynchronize(s));
+    cur = nx;
+    if (per_energy) {
+      int remaining = 0;
+      bool changed = false;
+      for (int64_t b = 0; b < batch; ++b) {
+        if (!hactive[b]) continue;
+        if (hdelta[b] < tol) {
+          hactive[b] = 0;
+          changed = true;
+        } else {
+          ++remaining;
+        }
+      }
+      if (remaining == 0) done = true;
+      if (changed && !done)
+        QTX_CHECK_CUDA(cudaMemcpyAsync(active, hactive.data(), sizeof(int) * batch,
+                                       cudaMemcpyHostToDevice, s));
+    } else {
+      double mx = 0.0;
+      for (int64_t b = 0; b < batch; ++b) mx = std::max(mx, hdelta[b]);
+      if (mx < tol) done = true;
+    }
+  }
+  if (iterations) *iterations = it;
+  if (converged) *converged = done ? 1 : 0;
+  if (delta_out) QTX_CHECK_CUDA(cudaMemcpyAsync(delta_out, delta, sizeof(double) * batch,
+                                                cudaMemcpyDeviceToDevice, s));
+  QTX_TRY(zinv(n, batch, eps_s, x, info, nullptr, s));
+  if (per_energy) QTX_CHECK_CUDA(cudaStreamSynchronize(s));  // hactive/hdelta stay valid until here
+  return QTX_OK;
+}
+
+size_t obc_refine_ws(int n, int64_t batch) {
+  Workspace ws;
+  for (int k = 0; k < 2; ++k) ws.mat(n, n, batch);
+  return ws.off + 256;
+}
+
+int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x, MatRef xref,
+                   double* rel, double* abs_res, int* info, Workspace& ws, cudaStream_t s) {
+  MatRef T = ws.mat(n, n, batch), S = ws.mat(n, n, batch);
+  if (ws.overflow) {
+    set_error("obc_refine: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  QTX_TRY(G(n, n, n, batch, aji, x, T).run(s));
+  QTX_TRY(G(n, n, n, batch, T, aij, S, MONE).plus(aii, ONE).run(s));
+  QTX_TRY(zinv(n, batch, S, S, info, nullptr, s));
+  QTX_TRY(znorm_diff(n, batch, S, x, abs_res, nullptr, rel, s));
+  Addend t{S, ONE, 0};
+  QTX_TRY(zcombine(n, n, batch, xref, &t, 1, nullptr, s));
+  return QTX_OK;
+}
+
+size_t contact_ws(int n, int64_t batch) {
+  Workspace ws;
+  ws.mat(n, n, batch);
+  ws.mat(n, n, batch);
+  return ws.off + 256;
+}
+
+int contact_run(int n, int64_t batch, MatRef aij, MatRef aji, MatRef g, const double* occ,
+                MatRef sigma, MatRef sl, MatRef sg, Workspace& ws, cudaStream_t s) {
+  MatRef T = ws.mat(n, n, batch);
+  MatRef Sg = sigma.null() ? ws.mat(n, n, batch) : sigma;
+  if (ws.overflow) {
+    set_error("contact_self_energy: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  QTX_TRY(G(n, n, n, batch, aji, g, T).run(s));
+  QTX_TRY(G(n, n, n, batch, T, aij, Sg).run(s));
+  if (!sl.null() || !sg.null()) {
+    if (occ == nullptr) {
+      set_error("contact_self_energy: occupancies required for lesser/greater outputs");
+      return QTX_ERR_ARG;
+    }
+    dim3 grid((n + 31) / 32, (n + 31) / 32, (unsigned)std::min<int64_t>(batch, 65535));
+    ProfScope prof(QTX_KERNEL_BLOCKOPS, 48.0 * n * n * (double)batch, s);
+    gamma_scale_kernel<<<grid, dim3(32, 8), 0, s>>>(n, batch, Sg, occ, sl, sg);
+    QTX_CHECK_LAUNCH();
+  }
+  return QTX_OK;
+}
+
+size_t transmission_ws(int m, int n, int64_t batch) {
+  Workspace ws;
+  const int bm = std::max(m, n);
+  for (int k = 0; k < 4; ++k) ws.mat(bm, bm, batch);
+  return ws.off + 256;
+}
+
+int transmission_run(int m, int n, int64_t batch, MatRef g0n, MatRef sl, MatRef sr, double* T,
+                     Workspace& ws, cudaStream_t s) {
+  const int bm = std::max(m, n);
+  MatRef GL = ws.mat(bm, bm, batch), GR = ws.mat(bm, bm, batch);
+  MatRef P1 = ws.mat(bm, bm, batch), P2 = ws.mat(bm, bm, batch);
+  if (ws.overflow) {
+    set_error("transmission: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  GL.ld = m;
+  GR.ld = n;
+  P1.ld = n;
+  P2.ld = n;
+  const z64 I{0.0, 1.0}, MI{0.0, -1.0};
+  Addend tl[2] = {Addend{sl, I, 0}, Addend{sl, MI, 1}};
+  QTX_TRY(zcombine(m, m, batch, GL, tl, 2, nullptr, s));
+  Addend tr[2] = {Addend{sr, I, 0}, Addend{sr, MI, 1}};
+  QTX_TRY(zcombine(n, n, batch, GR, tr, 2, nullptr, s));
+  QTX_TRY(G(m, n, m, batch, GL, g0n, P1).run(s));
+  QTX_TRY(G(m, n, n, batch, P1, GR, P2).run(s));
+  QTX_TRY(zre_inner(m, n, batch, P2, g0n, T, s));
+  return QTX_OK;
+}
+
+}  // namespace qtx

@@ -1,0 +1,317 @@
+// Batched complex128 matrix inverse: blocked Gauss-Jordan with partial
+// pivoting, one CTA per matrix.
+//
+// Replaces the batched inverse of qttools kernels/linalg/inv.py:6-40
+// (numpy.linalg.inv on CPU; cupy.linalg.solve(a, I) -> cuBLAS batched
+// getrf/getrs on NVIDIA GPUs). Every diagonal Schur-complement block of the
+// RGF forward sweep and every Sancho-Rubio step inverts through here.
+//
+// Algorithm (in place in X, n x n, panel width NB):
+//   for each panel K = [k0, k0 + NB):
+//     1. stage the n x NB panel X[:, K] in shared memory;
+//     2. factor it column by column: pivot = argmax_{r >= k} |Re|+|Im|
+//        (LAPACK izamax measure), swap, scale the pivot row by 1/pivot
+//        (Smith's complex division), eliminate every other row. Afterwards
+//        the panel holds T[:, K], where T is the Gauss-Jordan transform of
+//        this panel: T = [A_KK^-1 ; -A_RK A_KK^-1] in block form;
+//     3. apply the panel's row swaps to all other columns (global memory);
+//     4. update every other column tile J:
+//          X[:, J] = [0 ; X[R, J]] + T[:, K] X[K, J]
+//        a n x |J| x NB complex GEMM on the FP64 tensor pipe (DMMA);
+//     5. write the panel back.
+//   Finally undo the column permutation (pivots applied in reverse order).
+// Total work n^3 complex multiply-adds = 8 n^3 real flops.
+#include "common.cuh"
+
+namespace qtx {
+namespace {
+
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int JW = 32;  // column-tile width of the trailing update
+
+__device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// 1 / (a + ib) by Smith's algorithm (avoids overflow of a^2 + b^2).
+__device__ __forceinline__ z64 zrecip(z64 z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    if (z.x == 0.0 && z.y == 0.0) return make_double2(0.0, 0.0);
+    const double r = z.y / z.x;
+    const double den = z.x + z.y * r;
+    return make_double2(1.0 / den, -r / den);
+  }
+  const double r = z.x / z.y;
+  const double den = z.x * r + z.y;
+  return make_double2(r / den, -1.0 / den);
+}
+
+__device__ __forceinline__ double cabs1(z64 z) { return fabs(z.x) + fabs(z.y); }
+
+template <int NB>
+struct Smem {
+  static constexpr int PS = NB + 4;  // panel row stride (= 4 mod 8 in 16 B units)
+  static constexpr int YS = JW + 2;  // Y row stride (= 2 mod 8)
+  static size_t bytes(int n) {
+    size_t s = (size_t)n * PS * sizeof(z64);  // panel
+    s += (size_t)NB * YS * sizeof(z64);       // Y tile
+    s += (size_t)2 * NB * sizeof(z64);        // scaled pivot row, old row k
+    s += (size_t)WARPS * (sizeof(double) + sizeof(int));
+    s += (size_t)2 * n * sizeof(int);  // pivot rows, column sources
+    return s + 64;
+  }
+};
+
+template <int NB>
+__global__ void __launch_bounds__(THREADS) zinv_kernel(int n, int64_t batch, MatRef A, MatRef X,
+                                                        int* info, const int* active) {
+  using S = Smem<NB>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  z64* P = reinterpret_cast<z64*>(smem_raw);
+  z64* Y = P + (size_t)n * S::PS;
+  z64* prow = Y + NB * S::YS;
+  z64* rowk = prow + NB;
+  double* red_v = reinterpret_cast<double*>(rowk + NB);
+  int* red_i = reinterpret_cast<int*>(red_v + WARPS);
+  int* pivrow = red_i + WARPS;
+  int* colsrc = pivrow + n;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane >> 2;
+  const int tq = lane & 3;
+
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    if (active != nullptr && active[b] == 0) continue;
+    const z64* a = at<const z64>(A, b);
+    z64* x = at<z64>(X, b);
+    const int64_t lda = A.ld, ldx = X.ld;
+    if (a != x) {
+      for (int64_t idx = tid; idx < (int64_t)n * n; idx += THREADS) {
+        const int r = (int)(idx / n), c = (int)(idx % n);
+        x[(int64_t)r * ldx + c] = a[(int64_t)r * lda + c];
+      }
+    }
+    int singular_at = 0;
+    __syncthreads();
+
+    for (int k0 = 0; k0 < n; k0 += NB) {
+      const int nbp = min(NB, n - k0);
+      // 1. Stage the panel (zero-padded to NB columns).
+      for (int idx = tid; idx < n * NB; idx += THREADS) {
+        const int r = idx / NB, c = idx % NB;
+        P[r * S::PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+
+      // 2. Factor the panel.
+      for (int kk = 0; kk < nbp; ++kk) {
+        const int k = k0 + kk;
+        double best = -1.0;
+        int besti = k;
+        for (int r = k + tid; r < n; r += THREADS) {
+          const double v = cabs1(P[r * S::PS + kk]);
+          if (v > best) {
+            best = v;
+            besti = r;
+          }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+          const int oi = __shfl_xor_sync(0xffffffffu, besti, off);
+          if (ov > best || (ov == best && oi < besti)) {
+            best = ov;
+            besti = oi;
+          }
+        }
+        if (lane == 0) {
+          red_v[warp] = best;
+          red_i[warp] = besti;
+        }
+        __syncthreads();
+        best = red_v[0];
+        besti = red_i[0];
+#pragma unroll
+        for (int w = 1; w < WARPS; ++w) {
+          const double ov = red_v[w];
+          const int oi = red_i[w];
+          if (ov > best || (ov == best && oi < besti)) {
+            best = ov;
+            besti = oi;
+          }
+        }
+        const int p = besti;
+        if (best == 0.0 && singular_at == 0) singular_at = k + 1;
+        // Nobody writes P in this phase, so every thread can read the pivot.
+        const z64 dpiv = zrecip(P[p * S::PS + kk]);
+        if (tid < NB) {
+          const int c = tid;
+          rowk[c] = P[k * S::PS + c];
+          prow[c] = (c == kk) ? dpiv : zmul(P[p * S::PS + c], dpiv);
+        }
+        if (tid == 0) pivrow[k] = p;
+        __syncthreads();
+        // Eliminate; rows k and p are swapped on the fly (row p receives the
+        // old row k, row k becomes the scaled pivot row).
+        for (int r = tid; r < n; r += THREADS) {
+          if (r == k) {
+            for (int c = 0; c < NB; ++c) P[r * S::PS + c] = prow[c];
+            continue;
+          }
+          const z64* src = (r == p) ? rowk : P + r * S::PS;
+          const z64 f = src[kk];
+          for (int c = 0; c < NB; ++c) {
+            if (c == kk) continue;
+            const z64 v = src[c];
+            P[r * S::PS + c] = make_double2(v.x - (f.x * prow[c].x - f.y * prow[c].y),
+                                            v.y - (f.x * prow[c].y + f.y * prow[c].x));
+          }
+          const z64 m = zmul(f, dpiv);
+          P[r * S::PS + kk] = make_double2(-m.x, -m.y);
+        }
+        __syncthreads();
+      }
+
+      // 3. Apply the panel's row swaps to every column outside the panel.
+      for (int kk = 0; kk < nbp; ++kk) {
+        const int k = k0 + kk;
+        const int p = pivrow[k];
+        if (p != k) {
+          for (int c = tid; c < n; c += THREADS) {
+            if (c >= k0 && c < k0 + nbp) continue;
+            const z64 t = x[(int64_t)k * ldx + c];
+            x[(int64_t)k * ldx + c] = x[(int64_t)p * ldx + c];
+            x[(int64_t)p * ldx + c] = t;
+          }
+        }
+        __syncthreads();
+      }
+
+      // 4. Trailing update of every other column tile.
+      for (int j0 = 0; j0 < n; j0 += JW) {
+        // Columns of the panel itself are computed but never stored.
+        if (j0 >= k0 && j0 + JW <= k0 + nbp) continue;
+        for (int idx = tid; idx < NB * JW; idx += THREADS) {
+          const int kk = idx / JW, c = idx % JW;
+          Y[kk * S::YS + c] = (kk < nbp && j0 + c < n) ? x[(int64_t)(k0 + kk) * ldx + j0 + c]
+                                                      : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        const int mtiles = (n + 15) / 16;
+        for (int mt = warp; mt < mtiles; mt += WARPS) {
+          const int r0 = mt * 16;
+          double cre[JW / 8][4], cim[JW / 8][4];
+#pragma unroll
+          for (int j = 0; j < JW / 8; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int r = r0 + g + ((q >> 1) << 3);
+              const int c = j0 + j * 8 + 2 * tq + (q & 1);
+              z64 v = make_double2(0.0, 0.0);
+              if (r < n && c < n && !(r >= k0 && r < k0 + nbp) && (c < k0 || c >= k0 + nbp))
+                v = x[(int64_t)r * ldx + c];
+              cre[j][q] = v.x;
+              cim[j][q] = v.y;
+            }
+#pragma unroll
+          for (int k4 = 0; k4 < NB; k4 += 4) {
+            const int ra = r0 + g;
+            const z64 v0 = (ra < n) ? P[ra * S::PS + k4 + tq] : make_double2(0, 0);
+            const z64 v1 = (ra + 8 < n) ? P[(ra + 8) * S::PS + k4 + tq] : make_double2(0, 0);
+            const double nai0 = -v0.y, nai1 = -v1.y;
+#pragma unroll
+            for (int j = 0; j < JW / 8; ++j) {
+              const z64 bv = Y[(k4 + tq) * S::YS + j * 8 + g];
+              mma_f64(cre[j], v0.x, v1.x, bv.x);
+              mma_f64(cre[j], nai0, nai1, bv.y);
+              mma_f64(cim[j], v0.x, v1.x, bv.y);
+              mma_f64(cim[j], v0.y, v1.y, bv.x);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < JW / 8; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int r = r0 + g + ((q >> 1) << 3);
+              const int c = j0 + j * 8 + 2 * tq + (q & 1);
+              if (r < n && c < n && (c < k0 || c >= k0 + nbp))
+                x[(int64_t)r * ldx + c] = make_double2(cre[j][q], cim[j][q]);
+            }
+        }
+        __syncthreads();
+      }
+
+      // 5. Write the panel back.
+      for (int idx = tid; idx < n * nbp; idx += THREADS) {
+        const int r = idx / nbp, c = idx % nbp;
+        x[(int64_t)r * ldx + k0 + c] = P[r * S::PS + c];
+      }
+      __syncthreads();
+    }
+
+    // Undo the column permutation: swaps applied from the last pivot back.
+    if (tid == 0) {
+      for (int c = 0; c < n; ++c) colsrc[c] = c;
+      for (int k = n - 1; k >= 0; --k) {
+        const int p = pivrow[k];
+        if (p != k) {
+          const int t = colsrc[k];
+          colsrc[k] = colsrc[p];
+          colsrc[p] = t;
+        }
+      }
+    }
+    __syncthreads();
+    // Row-wise gather through the (now free) panel buffer, one warp per row.
+    z64* rowbuf = P + (size_t)warp * n;
+    for (int r = warp; r < n; r += WARPS) {
+      for (int c = lane; c < n; c += 32) rowbuf[c] = x[(int64_t)r * ldx + colsrc[c]];
+      __syncwarp();
+      for (int c = lane; c < n; c += 32) x[(int64_t)r * ldx + c] = rowbuf[c];
+      __syncwarp();
+    }
+    // Report the first singular block seen for this stack entry (callers
+    // zero `info` once per entry point).
+    if (tid == 0 && info != nullptr && singular_at != 0 && info[b] == 0) info[b] = singular_at;
+    __syncthreads();
+  }
+}
+
+template <int NB>
+int launch(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s) {
+  const size_t smem = Smem<NB>::bytes(n);
+  if (smem > 227 * 1024) {
+    set_error("zinv: block size too large for the shared-memory panel");
+    return QTX_ERR_UNSUPPORTED;
+  }
+  QTX_CHECK_CUDA(
+      cudaFuncSetAttribute(zinv_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned grid = (unsigned)(batch < 1048576 ? batch : 1048576);
+  ProfScope prof(QTX_KERNEL_ZINV, 8.0 * (double)n * n * n * (double)batch, s);
+  zinv_kernel<NB><<<grid, THREADS, smem, s>>>(n, batch, A, X, info, active);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+}  // namespace
+
+int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s) {
+  if (n <= 0 || batch <= 0) return QTX_OK;
+  if (A.null() || X.null()) {
+    set_error("zinv: null matrix");
+    return QTX_ERR_ARG;
+  }
+  if (n <= 512) return launch<16>(n, batch, A, X, info, active, s);
+  if (n <= 1024) return launch<8>(n, batch, A, X, info, active, s);
+  set_error("zinv: block sizes above 1024 are not supported");
+  return QTX_ERR_UNSUPPORTED;
+}
+
+}  // namespace qtx

@@ -1,0 +1,234 @@
+"""The per-energy NEGF unit of work on resident device data.
+
+One *energy point* is what ``ElectronSolver.solve``
+(``src/quatrex/electron/solver.py:756-888``) does per energy with zero
+scattering self-energy:
+
+1. assemble ``A(E) = (E + i eta) I - H`` (solver.py:668-709);
+2. both contacts: Sancho-Rubio surface Green's function
+   (``qttools/boundary_conditions/obc/sancho_rubio.py:33-85``) followed by the
+   ``OBCSystem`` residual/refinement step (``boundary_system.py:303-373``),
+   then ``Sigma = a_ji g a_ij``, ``Sigma^< = i f Gamma``,
+   ``Sigma^> = i (f - 1) Gamma`` (solver.py:420-495);
+3. ``RGF.selected_solve`` for G^R, G^<, G^> with the Meir-Wingreen current
+   (``qttools/greens_function_solver/rgf.py:115-438``);
+4. the Caroli transmission and the density Im diag G^<
+   (``quatrex/core/observables.py:8-31``).
+
+The Hamiltonian blocks stay resident on the GPU; energy-independent blocks
+(the couplings and the zero scattering self-energy blocks) are single
+blocks shared by the whole batch (stack stride 0), and every product is
+still executed as in the general solver. Output block stacks are allocated
+once per batch size and reused.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native
+from ._interop import mat
+from ._native import NULL_MAT, QtxBT, QtxMat
+from .obc import SanchoRubio, fixed_point_refine
+from .utils import workspace_pool
+
+_C128 = torch.complex128
+
+
+def _bcast(t: torch.Tensor) -> QtxMat:
+    """A single (b, b) block seen as a stack with stride 0."""
+    return QtxMat(t.data_ptr(), t.shape[-1], 0)
+
+
+@dataclass
+class PointResult:
+    transmission: torch.Tensor  # (B,) float64
+    density: torch.Tensor  # (B, N*b) float64
+    current: torch.Tensor  # (B, N+1) complex128
+    sigma_left: torch.Tensor
+    sigma_right: torch.Tensor
+    sr_iterations: tuple
+    blocks: dict = field(default_factory=dict)
+
+
+class EnergyPointSolver:
+    """Solves batches of energy points of one block-tridiagonal device.
+
+    Parameters
+    ----------
+    h_diag : (N, b, b) complex array
+        Diagonal Hamiltonian blocks.
+    coupling : (b, b) complex array
+        Block (i, i+1) of H; block (i+1, i) is its adjoint.
+    eta : float
+        Broadening in ``A = (E + i eta) I - H``.
+    sr_tol, sr_max_iterations : Sancho-Rubio stop criterion.
+    per_energy : bool
+        Per-energy Sancho-Rubio convergence (converged energies stop
+        iterating) instead of the batch-wide stop.
+    skip_zero_scattering : bool
+        False (default): the zero scattering self-energy is passed as zero
+        blocks and every product of the general solve is executed, as in the
+        reference. True: it is passed as absent and the products with it are
+        skipped (ballistic shortcut).
+    """
+
+    def __init__(self, h_diag, coupling, eta: float = 1e-4, sr_tol: float = 1e-12,
+                 sr_max_iterations: int = 100, per_energy: bool = True,
+                 skip_zero_scattering: bool = False, device: torch.device | None = None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        h = torch.as_tensor(np.asarray(h_diag), dtype=_C128) if not isinstance(h_diag, torch.Tensor) else h_diag
+        t = torch.as_tensor(np.asarray(coupling), dtype=_C128) if not isinstance(coupling, torch.Tensor) else coupling
+        self.h = h.to(self.device, _C128).contiguous()
+        self.N, self.b = int(self.h.shape[0]), int(self.h.shape[-1])
+        self.upper = (-t).to(self.device, _C128).contiguous()
+        self.lower = (-t.conj().transpose(-2, -1)).to(self.device, _C128).contiguous()
+        self.zero = torch.zeros((self.b, self.b), dtype=_C128, device=self.device)
+        self.eta = float(eta)
+        self.sr = SanchoRubio(max_iterations=sr_max_iterations, convergence_tol=sr_tol,
+                              per_energy=per_energy)
+        self.skip_zero_scattering = skip_zero_scattering
+        self._bufs: dict = {}
+        self.lib = _native.load()
+
+    # ------------------------------------------------------------------
+    def _buffers(self, B: int) -> dict:
+        buf = self._bufs.get(B)
+        if buf is not None:
+            return buf
+        N, b, dev = self.N, self.b, self.device
+        z = lambda *s: torch.empty(s, dtype=_C128, device=dev)  # noqa: E731
+        buf = dict(
+            a_diag=z(N, B, b, b), xl_d=z(N, B, b, b), xl_u=z(max(N - 1, 1), B, b, b),
+            xl_l=z(max(N - 1, 1), B, b, b), xg_d=z(N, B, b, b), xg_u=z(max(N - 1, 1), B, b, b),
+            xg_l=z(max(N - 1, 1), B, b, b), xr_d=z(N, B, b, b), g0n=z(B, b, b),
+            gl=z(B, b, b), gr=z(B, b, b), sig=[z(B, b, b) for _ in range(6)],
+            current=z(B, N + 1), density=torch.empty((B, N * b), dtype=torch.float64, device=dev),
+            T=torch.empty(B, dtype=torch.float64, device=dev), zE=z(B),
+            info=torch.zeros(B, dtype=torch.int32, device=dev),
+        )
+        self._bufs = {B: buf}  # keep one batch size resident
+        return buf
+
+    def _bt(self, diag, upper, lower, keep):
+        n = self.N
+        bs = (ctypes.c_int32 * n)(*([self.b] * n))
+        d = (QtxMat * n)(*diag)
+        u = (QtxMat * max(n - 1, 1))(*(upper or [NULL_MAT]))
+        lo = (QtxMat * max(n - 1, 1))(*(lower or [NULL_MAT]))
+        keep.extend([bs, d, u, lo])
+        return QtxBT(n, bs, d, u, lo)
+
+    # ------------------------------------------------------------------
+    def solve(self, energies, f_left, f_right) -> PointResult:
+        """Solves one batch of energies; all results stay on the device."""
+        lib, dev = self.lib, self.device
+        N, b = self.N, self.b
+        E = torch.as_tensor(energies, dtype=torch.float64, device=dev).reshape(-1)
+        B = int(E.numel())
+        buf = self._buffers(B)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        buf["zE"].copy_(E.to(_C128) + 1j * self.eta)
+        fl = torch.as_tensor(f_left, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+        fr = torch.as_tensor(f_right, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+
+        # 1. A(E) diagonal blocks.
+        a_diag = buf["a_diag"]
+        for i in range(N):
+            _native.check(lib.qtx_assemble_diag(b, B, _bcast(self.h[i]), buf["zE"].data_ptr(),
+                                                mat(a_diag[i]), stream))
+
+        # 2. Boundary conditions, left = (A00, A01, A10), right =
+        #    (A_NN, A_N,N-1, A_N-1,N).
+        up, lo = _bcast(self.upper), _bcast(self.lower)
+        sig = buf["sig"]
+        iters = []
+        for side, (aii, aij, aji, g, f, s3) in enumerate((
+                (a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
+                (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))):
+            x, it, conv = self._sr(aii, aij, aji, g)
+            iters.append(it)
+            if not conv:
+                warnings.warn("Surface Green's function did not converge.", RuntimeWarning)
+            self._refine(aii, aij, aji, g, B, stream)
+            ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
+            _native.check(lib.qtx_contact_self_energy(b, B, aij, aji, mat(g), f.data_ptr(), mat(s3[0]),
+                                                      mat(s3[1]), mat(s3[2]), ws.data_ptr(), ws.numel(),
+                                                      stream))
+
+        # 3. Selected solve.
+        keep: list = []
+        A = self._bt([mat(a_diag[i]) for i in range(N)], [up] * (N - 1), [lo] * (N - 1), keep)
+        zs = NULL_MAT if self.skip_zero_scattering else _bcast(self.zero)
+        S = self._bt([zs] * N, [zs] * (N - 1), [zs] * (N - 1), keep)
+        XL = self._bt([mat(buf["xl_d"][i]) for i in range(N)], [mat(buf["xl_u"][i]) for i in range(N - 1)],
+                      [mat(buf["xl_l"][i]) for i in range(N - 1)], keep)
+        XG = self._bt([mat(buf["xg_d"][i]) for i in range(N)], [mat(buf["xg_u"][i]) for i in range(N - 1)],
+                      [mat(buf["xg_l"][i]) for i in range(N - 1)], keep)
+        XR = self._bt([mat(buf["xr_d"][i]) for i in range(N)], [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1), keep)
+        obc = []
+        for k in range(3):
+            arr = (QtxMat * N)(*([NULL_MAT] * N))
+            arr[0] = mat(sig[k])
+            arr[N - 1] = mat(sig[3 + k]) if N > 1 else arr[0]
+            obc.append(arr)
+        if N == 1:
+            raise ValueError("EnergyPointSolver needs at least two blocks")
+        ws_bytes = lib.qtx_selected_solve_workspace(N, A.block_sizes, B, 1)
+        ws = workspace_pool.get(ws_bytes, dev, "rgf")
+        _native.check(lib.qtx_selected_solve(
+            ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
+            ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
+            buf["density"].data_ptr(), 0, B, buf["info"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
+
+        # 4. Transmission.
+        ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
+        _native.check(lib.qtx_transmission(b, b, B, mat(buf["g0n"]), mat(sig[0]), mat(sig[3]),
+                                           buf["T"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
+        blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
+                      xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
+        return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], tuple(iters), blocks)
+
+    def _sr(self, aii, aij: QtxMat, aji: QtxMat, out):
+        lib, dev = self.lib, self.device
+        B = aii.shape[0]
+        ws = workspace_pool.get(lib.qtx_sancho_rubio_workspace(self.b, B), dev, "sr")
+        it, conv = ctypes.c_int(0), ctypes.c_int(0)
+        _native.check(lib.qtx_sancho_rubio(
+            self.b, B, mat(aii), aij, aji, mat(out), int(self.sr.max_iterations),
+            float(self.sr.convergence_tol), int(self.sr.per_energy), ctypes.byref(it), ctypes.byref(conv),
+            None, None, ws.data_ptr(), ws.numel(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+        return out, it.value, bool(conv.value)
+
+    def _refine(self, aii, aij: QtxMat, aji: QtxMat, g, B, stream):
+        lib, dev = self.lib, self.device
+        ws = workspace_pool.get(lib.qtx_obc_workspace(self.b, B), dev, "obc")
+        rel = torch.empty(B, dtype=torch.float64, device=dev)
+        ab = torch.empty(B, dtype=torch.float64, device=dev)
+        _native.check(lib.qtx_obc_refine(self.b, B, mat(aii), aij, aji, mat(g), mat(g), rel.data_ptr(),
+                                         ab.data_ptr(), None, ws.data_ptr(), ws.numel(), stream))
+        self.last_residuals = (rel, ab)
+
+
+def flops_per_energy(N: int, b: int, sr_iterations: tuple = (0, 0)) -> dict:
+    """Reference ("as written") real-flop counts of one energy point:
+    a complex b x b x b product = 8 b^3 flops, a complex inverse = 8 b^3.
+
+    F_solve = 8b^3 [N + 4 + 33(N-1)]   (rgf.py:234-238,272-301,334-410)
+    F_cur   = 8b^3 [9(N-1) + 4]        (rgf.py:389-428)
+    F_SR    = 8b^3 [11K + 1] per contact (sancho_rubio.py:64-83)
+    F_obc   = 8b^3 [3 + 2] per contact (refinement step + sigma product)
+    """
+    u = 8.0 * b ** 3
+    f_solve = u * (N + 4 + 33 * (N - 1))
+    f_cur = u * (9 * (N - 1) + 4)
+    f_sr = sum(u * (11 * k + 1) for k in sr_iterations)
+    f_obc = 2 * u * 5
+    f_trans = u * 2
+    return dict(solve=f_solve, current=f_cur, sr=f_sr, obc=f_obc, transmission=f_trans,
+                total=f_solve + f_cur + f_sr + f_obc + f_trans)

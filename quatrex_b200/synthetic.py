@@ -1,0 +1,185 @@
+"""Seeded synthetic transport devices for the NEGF hot path.
+
+The device is a block-tridiagonal tight-binding Hamiltonian with ``N``
+diagonal blocks of size ``b``:
+
+* ``H_ii = (M_i + M_i^H) / 2`` with ``M_i = (X + iY) / 8`` and X, Y standard
+  normal ``b x b`` draws;
+* one coupling ``T = (X + iY) / 8`` shared by every ``(i, i+1)`` pair, with
+  ``H_{i+1,i} = T^H``.
+
+Draw order (``numpy.random.default_rng(seed)``): for ``i = 0..N-1`` the real
+part then the imaginary part of ``M_i``; then the real part then the
+imaginary part of ``T``. The leads repeat the first and last block pair, so
+the open-boundary blocks are taken from the system matrix itself (the
+``block_sections == 1`` case of qttools' ``get_periodic_superblocks``,
+``src/qttools/toeplitz/toeplitz.py:76-77``).
+
+The system matrix at energy ``E`` is ``A(E) = (E + i eta) I - H`` and the
+contact occupations follow the Fermi function ``f(x) = 1 / (1 + exp(x/kT))``
+with ``f_L(E) = f(E)``, ``f_R(E) = f(E - bias)``
+(``src/quatrex/core/statistics.py:7-23``).
+
+Configurations (sizes of the reference benchmark workloads):
+
+=====  ====  ====  =========  ==============
+name    N     b    energies    energy window
+=====  ====  ====  =========  ==============
+cfg0    16    64       32       [-2, 2]
+cfg1    32   256     1024       [-3, 3]
+cfg2    64   512     2048       [-3, 3]
+=====  ====  ====  =========  ==============
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+ETA = 1e-4
+KT = 0.025
+BIAS = 0.1
+
+
+@dataclass
+class Device:
+    """A block-tridiagonal device Hamiltonian (host, complex128)."""
+
+    h_diag: np.ndarray  # (N, b, b)
+    coupling: np.ndarray  # (b, b): block (i, i+1); block (i+1, i) is its adjoint
+    energies: np.ndarray  # (E,)
+    eta: float = ETA
+    kT: float = KT
+    bias: float = BIAS
+    name: str = "custom"
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_blocks(self) -> int:
+        return int(self.h_diag.shape[0])
+
+    @property
+    def block_size(self) -> int:
+        return int(self.h_diag.shape[1])
+
+    @property
+    def block_sizes(self) -> np.ndarray:
+        return np.full(self.num_blocks, self.block_size, dtype=np.int64)
+
+    def fermi_left(self, energies: np.ndarray | None = None) -> np.ndarray:
+        e = self.energies if energies is None else np.asarray(energies)
+        return fermi(e, self.kT)
+
+    def fermi_right(self, energies: np.ndarray | None = None) -> np.ndarray:
+        e = self.energies if energies is None else np.asarray(energies)
+        return fermi(e - self.bias, self.kT)
+
+    def system_blocks(self, energies: np.ndarray | None = None):
+        """Dense blocks of ``A(E) = (E + i eta) I - H`` for the given energies.
+
+        Returns ``(diag, upper, lower)`` lists: ``diag[i]`` has shape
+        ``(E, b, b)``; ``upper[i]`` is block ``(i, i+1)``; ``lower[i]`` is
+        block ``(i+1, i)``.
+        """
+        e = self.energies if energies is None else np.asarray(energies)
+        z = (e + 1j * self.eta).astype(np.complex128)
+        b = self.block_size
+        eye = np.eye(b, dtype=np.complex128)
+        diag = [z[:, None, None] * eye - self.h_diag[i][None] for i in range(self.num_blocks)]
+        up = np.broadcast_to(-self.coupling, (e.size, b, b)).copy()
+        lo = np.broadcast_to(-self.coupling.conj().T, (e.size, b, b)).copy()
+        upper = [up.copy() for _ in range(self.num_blocks - 1)]
+        lower = [lo.copy() for _ in range(self.num_blocks - 1)]
+        return diag, upper, lower
+
+    def dense_hamiltonian(self) -> np.ndarray:
+        n, b = self.num_blocks, self.block_size
+        h = np.zeros((n * b, n * b), dtype=np.complex128)
+        for i in range(n):
+            h[i * b:(i + 1) * b, i * b:(i + 1) * b] = self.h_diag[i]
+            if i + 1 < n:
+                h[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = self.coupling
+                h[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = self.coupling.conj().T
+        return h
+
+
+def fermi(x: np.ndarray, kT: float) -> np.ndarray:
+    """Fermi-Dirac occupation ``1 / (1 + exp(x / kT))`` (x in eV)."""
+    return 1.0 / (1.0 + np.exp(np.asarray(x, dtype=np.float64) / kT))
+
+
+def make_device(num_blocks: int, block_size: int, energies: np.ndarray, seed: int = 0,
+                name: str = "custom") -> Device:
+    """Builds the seeded random device described in the module docstring."""
+    rng = np.random.default_rng(seed)
+    b = int(block_size)
+    h = np.empty((num_blocks, b, b), dtype=np.complex128)
+    for i in range(num_blocks):
+        re = rng.standard_normal((b, b))
+        im = rng.standard_normal((b, b))
+        m = (re + 1j * im) / 8.0
+        h[i] = 0.5 * (m + m.conj().T)
+    re = rng.standard_normal((b, b))
+    im = rng.standard_normal((b, b))
+    t = (re + 1j * im) / 8.0
+    return Device(h_diag=h, coupling=t, energies=np.asarray(energies, dtype=np.float64), name=name)
+
+
+def cfg0() -> Device:
+    """16 blocks of 64x64, 32 energies uniform in [-2, 2], seed 0."""
+    return make_device(16, 64, np.linspace(-2.0, 2.0, 32), seed=0, name="cfg0")
+
+
+def cfg1(num_energies: int = 1024) -> Device:
+    """32 blocks of 256x256, 1024 energies uniform in [-3, 3], seed 0."""
+    return make_device(32, 256, np.linspace(-3.0, 3.0, num_energies), seed=0, name="cfg1")
+
+
+def cfg2(num_energies: int = 2048) -> Device:
+    """64 blocks of 512x512, 2048 energies uniform in [-3, 3], seed 0."""
+    return make_device(64, 512, np.linspace(-3.0, 3.0, num_energies), seed=0, name="cfg2")
+
+
+def uneven_devices(num_devices: int = 8, num_energies: int = 256, seed: int = 1,
+                   block_counts=(8, 16, 32, 64), block_sizes=(128, 256, 384, 512, 768)):
+    """The uneven batch: per device, N then b drawn uniformly with
+    ``default_rng(seed)``; each device is then built like :func:`cfg0` (seed
+    0 Hamiltonian construction with its own N, b) on ``num_energies`` energies
+    uniform in [-2, 2]."""
+    rng = np.random.default_rng(seed)
+    shapes = []
+    for _ in range(num_devices):
+        n = int(rng.choice(block_counts))
+        b = int(rng.choice(block_sizes))
+        shapes.append((n, b))
+    return shapes
+
+
+def random_bt_dense(block_sizes, seed: int = 0, density: float = 0.5) -> np.ndarray:
+    """Quasi-sparse, diagonally dominant random block-tridiagonal matrix.
+
+    Same construction as the qttools GF-solver test fixture
+    (``tests/qttools/greens_function_solver/conftest.py:58-104``), with a
+    seeded generator so the case is reproducible.
+    """
+    rng = np.random.default_rng(seed)
+    block_sizes = np.asarray(block_sizes, dtype=np.int64)
+    offs = np.concatenate(([0], np.cumsum(block_sizes)))
+    size = int(offs[-1])
+    arr = np.zeros((size, size), dtype=np.complex128)
+
+    def rblock(m, n):
+        mask = rng.random((m, n)) < density
+        vals = rng.random((m, n)) + 1j * rng.random((m, n))
+        return np.where(mask, vals, 0.0)
+
+    for i in range(len(block_sizes)):
+        arr[offs[i]:offs[i + 1], offs[i]:offs[i + 1]] = rblock(block_sizes[i], block_sizes[i]) + np.eye(
+            block_sizes[i])
+        if i > 0:
+            arr[offs[i]:offs[i + 1], offs[i - 1]:offs[i]] = rblock(block_sizes[i], block_sizes[i - 1])
+            arr[offs[i - 1]:offs[i], offs[i]:offs[i + 1]] = rblock(block_sizes[i - 1], block_sizes[i])
+    for i in range(size):
+        arr[i, i] = (1 + 1j) + arr[i, :].sum()
+    return arr
