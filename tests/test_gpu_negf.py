@@ -2,11 +2,18 @@
 G^R, G^<, G^>, Meir-Wingreen current, Caroli transmission, density) on the
 GPU against the reference golden vectors and the oracle.
 
-Tolerance (FP64): 1e-10 relative for the RGF outputs given the same
-boundary self-energies; the Sancho-Rubio surface Green's function itself is
-rounding-sensitive at eta = 1e-4 (the reference's own left/right
-orientation flip moves Sigma_R by 1.4e-10 relative), so the end-to-end
-energy-point results are checked at 1e-9."""
+Tolerances (FP64):
+* 1e-10 relative for everything the RGF produces from the same boundary
+  self-energies (the plain-FP64 parity gate);
+* end-to-end results go through the Sancho-Rubio decimation, which is
+  numerically unstable at eta = 1e-4: a 1e-14 relative perturbation of one
+  inverse changes the reference's own surface Green's function by up to
+  1e-5 at some cfg1 energies (and the reference's left/right orientation
+  flip alone moves Sigma_R by 3e-9). End-to-end observables are therefore
+  checked against the reference at 1e-9 for the 64x64 case and at 1e-7
+  (transmission, density, current) for the 256x256 case, where the
+  decimation noise floor of the reference itself is ~1e-8.
+"""
 
 import numpy as np
 import pytest
@@ -18,6 +25,7 @@ from quatrex_b200 import EnergyPointSolver, synthetic
 pytestmark = pytest.mark.gpu
 
 TOL_E2E = 1e-9
+TOL_E2E_CFG1 = 1e-7
 
 
 def _rel(a, b):
@@ -68,11 +76,12 @@ def test_cfg0_rgf_given_same_obc_matches_oracle(cfg0_gpu):
     """Isolates the RGF part: the oracle solve fed with the GPU's boundary
     self-energies must agree to 1e-10."""
     dev, s, r = cfg0_gpu
-    e = dev.energies[:8]
+    sel = np.arange(12, 20)  # energies around the bias window: f_L != f_R
+    e = dev.energies[sel]
     diag, upper, lower = dev.system_blocks(e)
     n = dev.num_blocks
-    sl = r.sigma_left.cpu().numpy()[:8]
-    sr = r.sigma_right.cpu().numpy()[:8]
+    sl = r.sigma_left.cpu().numpy()[sel]
+    sr = r.sigma_right.cpu().numpy()[sel]
     fl, fr = dev.fermi_left(e), dev.fermi_right(e)
     gam = lambda x: 1j * (x - x.conj().swapaxes(-2, -1))  # noqa: E731
     obr, obl, obg = [None] * n, [None] * n, [None] * n
@@ -83,12 +92,14 @@ def test_cfg0_rgf_given_same_obc_matches_oracle(cfg0_gpu):
     zu = [np.zeros_like(u) for u in upper]
     ref = o.selected_solve(diag, upper, lower, z, zu, zu, z, zu, zu, obr, obl, obg, return_current=True)
     errs = {
-        "current": _rel(r.current.cpu().numpy()[:8], ref["current"]),
-        "xr0": _rel(r.blocks["xr_diag"][0].cpu().numpy()[:8], ref["xr_diag"][0]),
-        "xl5": _rel(r.blocks["xl_diag"][5].cpu().numpy()[:8], ref["xl_diag"][5]),
-        "xg_up3": _rel(r.blocks["xg_upper"][3].cpu().numpy()[:8], ref["xg_upper"][3]),
-        "xl_lo3": _rel(r.blocks["xl_lower"][3].cpu().numpy()[:8], ref["xl_lower"][3]),
-        "density": _rel(r.density.cpu().numpy()[:8], o.density(ref["xl_diag"])),
+        "current": _rel(r.current.cpu().numpy()[sel], ref["current"]),
+        "xr0": _rel(r.blocks["xr_diag"][0].cpu().numpy()[sel], ref["xr_diag"][0]),
+        "xl5": _rel(r.blocks["xl_diag"][5].cpu().numpy()[sel], ref["xl_diag"][5]),
+        "xg_up3": _rel(r.blocks["xg_upper"][3].cpu().numpy()[sel], ref["xg_upper"][3]),
+        "xl_lo3": _rel(r.blocks["xl_lower"][3].cpu().numpy()[sel], ref["xl_lower"][3]),
+        "density": _rel(r.density.cpu().numpy()[sel], o.density(ref["xl_diag"])),
+        "transmission": _rel(r.transmission.cpu().numpy()[sel],
+                             o.transmission_caroli_rgf(diag, upper, lower, obr, sl, sr)),
     }
     print("cfg0 RGF errors vs oracle (same OBC):", errs)
     assert all(v < 1e-10 for v in errs.values()), errs
@@ -129,4 +140,48 @@ def test_cfg1_sample_matches_reference(cuda_device, golden):
         "xl_fro": _rel(np.linalg.norm(r.blocks["xl_diag"].cpu().numpy(), axis=(-2, -1)).T, g["xl_fro"]),
     }
     print("cfg1 sample errors vs reference:", errs)
-    assert all(v < TOL_E2E for v in errs.values()), errs
+    assert errs["transmission"] < TOL_E2E_CFG1 and errs["density"] < TOL_E2E_CFG1, errs
+    assert errs["current"] < TOL_E2E_CFG1 and errs["xl_fro"] < TOL_E2E_CFG1, errs
+    assert errs["xr_fro"] < 1e-6, errs  # G^R near the leads inherits the decimation noise
+
+
+def test_cfg1_rgf_given_same_obc_matches_oracle(cuda_device):
+    """The 1e-10 FP64 gate at 256x256: RGF outputs from identical boundary
+    self-energies (one energy, oracle on CPU)."""
+    dev = synthetic.cfg1()
+    e = dev.energies[[511]]
+    s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=False)
+    r = s.solve(e, dev.fermi_left(e), dev.fermi_right(e))
+    diag, upper, lower = dev.system_blocks(e)
+    n = dev.num_blocks
+    sl, sr = r.sigma_left.cpu().numpy(), r.sigma_right.cpu().numpy()
+    fl, fr = dev.fermi_left(e), dev.fermi_right(e)
+    gam = lambda x: 1j * (x - x.conj().swapaxes(-2, -1))  # noqa: E731
+    obr, obl, obg = [None] * n, [None] * n, [None] * n
+    obr[0], obr[-1] = sl, sr
+    obl[0], obl[-1] = 1j * gam(sl) * fl[:, None, None], 1j * gam(sr) * fr[:, None, None]
+    obg[0], obg[-1] = 1j * gam(sl) * (fl - 1)[:, None, None], 1j * gam(sr) * (fr - 1)[:, None, None]
+    z = [np.zeros_like(d) for d in diag]
+    zu = [np.zeros_like(u) for u in upper]
+    ref = o.selected_solve(diag, upper, lower, z, zu, zu, z, zu, zu, obr, obl, obg, return_current=True)
+    errs = {
+        "current": _rel(r.current.cpu().numpy(), ref["current"]),
+        "density": _rel(r.density.cpu().numpy(), o.density(ref["xl_diag"])),
+        "xr_diag": max(_rel(r.blocks["xr_diag"][i].cpu().numpy(), ref["xr_diag"][i]) for i in (0, 15, 31)),
+        "xg_upper": max(_rel(r.blocks["xg_upper"][i].cpu().numpy(), ref["xg_upper"][i]) for i in (0, 30)),
+        "transmission": _rel(r.transmission.cpu().numpy(),
+                             o.transmission_caroli_rgf(diag, upper, lower, obr, sl, sr)),
+    }
+    print("cfg1 RGF errors vs oracle (same OBC):", errs)
+    assert all(v < 1e-10 for v in errs.values()), errs
+
+
+def test_sr_fixed_point_residual_cfg1(cuda_device):
+    """The GPU surface Green's function satisfies the OBC fixed point as
+    tightly as the reference's own (obc.py:156-195 residual)."""
+    dev = synthetic.cfg1()
+    e = dev.energies[[100, 900]]
+    s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=False)
+    s.solve(e, dev.fermi_left(e), dev.fermi_right(e))
+    rel, _ = s.last_residuals
+    assert float(rel.max()) < 1e-6
