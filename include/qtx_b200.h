@@ -110,6 +110,18 @@ size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes
 int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x, int64_t batch,
                      int* info, void* workspace, size_t workspace_bytes, qtx_stream stream);
 
+/* qtx_selected_inv without a caller workspace and without any allocation:
+ * its scratch is a file-scope 64 MiB device array in the library (held by
+ * every GPU that loads it until exit). For callers that cannot call
+ * cudaMalloc/cudaFree during a solve (both synchronise the device and fail
+ * once another allocator owns the memory). Requests needing more than 64 MiB
+ * (sum_i b_i^2 + 6 b_max^2 complex128 per energy) return QTX_ERR_WORKSPACE.
+ * All calls share the array: calls that overlap on the GPU race. A device's
+ * first call resolves the array's device address; make it before any stream
+ * capture. This entry point has no counterpart in the reference. */
+int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x,
+                            int64_t batch, int* info, qtx_stream stream);
+
 /* Workspace bytes for qtx_selected_solve. */
 size_t qtx_selected_solve_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch,
                                     int return_current);

@@ -51,6 +51,8 @@ SIGNATURES = {
     "qtx_selected_inv_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64]),
     "qtx_selected_inv": (c_int, [POINTER(QtxBT), POINTER(QtxMat), POINTER(QtxBT), c_int64, c_void_p,
                                  c_void_p, c_size_t, c_void_p]),
+    "qtx_selected_inv_static": (c_int, [POINTER(QtxBT), POINTER(QtxMat), POINTER(QtxBT), c_int64, c_void_p,
+                                        c_void_p]),
     "qtx_selected_solve_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64, c_int]),
     "qtx_selected_solve": (c_int, [POINTER(QtxBT), POINTER(QtxBT), POINTER(QtxBT), POINTER(QtxMat),
                                    POINTER(QtxMat), POINTER(QtxMat), POINTER(QtxBT), POINTER(QtxBT),
