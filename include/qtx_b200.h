@@ -92,6 +92,14 @@ int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, doubl
                       qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re, double beta_im,
                       qtx_mat d, int op_d, qtx_mat c, qtx_stream stream);
 
+/* Batched complex64 GEMM on the tcgen05 tensor cores, split-TF32 products
+ * with FP32 accumulation (mixed precision path):
+ * C = alpha op(A) op(B) + beta op(D), complex64 interleaved. err: optional
+ * device int set to 1 if an internal wait timed out. */
+int qtx_cgemm_batched(int m, int n, int k, int64_t batch, float alpha_re, float alpha_im, qtx_mat a,
+                      int op_a, qtx_mat b, int op_b, float beta_re, float beta_im, qtx_mat d,
+                      int op_d, qtx_mat c, int* err, qtx_stream stream);
+
 /* Batched complex128 inverse X = A^{-1} (Gauss-Jordan, partial pivoting).
  * Replaces qttools/kernels/linalg/inv.py:6-40 (numpy.linalg.inv /
  * cupy.linalg.solve(a, I)). info: device int[batch], 0 or the 1-based
@@ -147,6 +155,27 @@ int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt
                        int flags, int64_t batch, int* info, void* workspace,
                        size_t workspace_bytes, qtx_stream stream);
 
+/* Workspace bytes for qtx_selected_solve_mixed. */
+size_t qtx_selected_solve_mixed_workspace(int32_t num_blocks, const int32_t* block_sizes,
+                                          int64_t batch, int return_current);
+
+/* qtx_selected_solve in mixed precision (QTX_MIXED): all block stacks are
+ * complex64; block products run on the tcgen05 tensor cores as split-TF32
+ * products with FP32 accumulation; every Schur-complement block is inverted
+ * in FP64 (upcast, Gauss-Jordan with partial pivoting, rounded back). The
+ * current and the density are accumulated in double. g0n is complex64. */
+int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
+                             const qtx_bt* sigma_greater, const qtx_mat* obc_retarded,
+                             const qtx_mat* obc_lesser, const qtx_mat* obc_greater, const qtx_bt* xl,
+                             const qtx_bt* xg, const qtx_bt* xr, void* current, qtx_mat g0n,
+                             double* density, int flags, int64_t batch, int* info, void* workspace,
+                             size_t workspace_bytes, qtx_stream stream);
+
+/* Converts an m x n stack between complex128 (QTX_C128) and complex64
+ * (QTX_C64), or copies it within one type. */
+int qtx_convert(int m, int n, int64_t batch, qtx_mat in, int in_dtype, qtx_mat out, int out_dtype,
+                qtx_stream stream);
+
 /* Workspace bytes for qtx_sancho_rubio. */
 size_t qtx_sancho_rubio_workspace(int n, int64_t batch);
 
@@ -164,6 +193,19 @@ int qtx_sancho_rubio(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a
                      int max_iterations, double tol, int per_energy, int* iterations,
                      int* converged, double* delta_out, int* info, void* workspace,
                      size_t workspace_bytes, qtx_stream stream);
+
+/* Sancho-Rubio on several systems of one block size in a single decimation
+ * loop (e.g. both contacts of a device, or the leads of several devices):
+ * system k has batches[k] entries with inputs a_ii[k], a_ij[k], a_ji[k] and
+ * output x[k]. The systems are concatenated, so every launch covers all of
+ * them. Workspace: qtx_sancho_rubio_workspace(n, sum(batches)). Stop
+ * criteria as qtx_sancho_rubio over the concatenated batch; info (device,
+ * optional) has sum(batches) entries in system order. */
+int qtx_sancho_rubio_multi(int n, int num_systems, const int64_t* batches, const qtx_mat* a_ii,
+                           const qtx_mat* a_ij, const qtx_mat* a_ji, const qtx_mat* x,
+                           int max_iterations, double tol, int per_energy, int* iterations,
+                           int* converged, int* info, void* workspace, size_t workspace_bytes,
+                           qtx_stream stream);
 
 /* Workspace bytes sufficient for qtx_contact_self_energy, qtx_obc_refine
  * and qtx_transmission (square n x n blocks) on `batch` entries. */
@@ -223,7 +265,8 @@ enum qtx_kernel_class {
   QTX_KERNEL_ZINV = 1,     /* batched inverse; work = 8 n^3 flops */
   QTX_KERNEL_BLOCKOPS = 2, /* elementwise block kernels; work = bytes */
   QTX_KERNEL_REDUCE = 3,   /* traces / norms; work = bytes */
-  QTX_KERNEL_FORMAT = 4    /* assembly, densify / sparsify; work = bytes */
+  QTX_KERNEL_FORMAT = 4,   /* assembly, densify / sparsify; work = bytes */
+  QTX_KERNEL_CGEMM = 5     /* complex64 tcgen05 GEMM (split TF32); work = 8 m n k flops */
 };
 /* Turns event bracketing of every library kernel launch on or off. */
 int qtx_profile_enable(int on);

@@ -96,13 +96,13 @@ def mat(t: torch.Tensor, offset_elems: int = 0, ld: int | None = None,
     (batch, nnz) data tensor starting at ``offset_elems``."""
     if t is None:
         return NULL_MAT
-    if t.dtype != _C128:
-        raise TypeError(f"expected complex128 device data, got {t.dtype}")
+    if t.dtype not in (_C128, torch.complex64):
+        raise TypeError(f"expected complex128 or complex64 device data, got {t.dtype}")
     if ld is None:
         ld = t.stride(-2)
     if stride is None:
-        stride = t.stride(0) if t.dim() >= 3 or offset_elems else t.stride(0)
-    return QtxMat(t.data_ptr() + offset_elems * _ELEM, int(ld), int(stride))
+        stride = t.stride(0)
+    return QtxMat(t.data_ptr() + offset_elems * t.element_size(), int(ld), int(stride))
 
 
 def stack3(x: torch.Tensor) -> torch.Tensor:

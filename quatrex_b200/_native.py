@@ -21,8 +21,10 @@ QTX_ERR_WORKSPACE = -3
 QTX_ERR_SINGULAR = -4
 QTX_ERR_UNSUPPORTED = -5
 QTX_SOLVE_SYMMETRIC_OUT = 1
+QTX_C128 = 0
+QTX_C64 = 1
 
-KERNEL_CLASSES = {"zgemm": 0, "zinv": 1, "blockops": 2, "reduce": 3, "format": 4}
+KERNEL_CLASSES = {"zgemm": 0, "zinv": 1, "blockops": 2, "reduce": 3, "format": 4, "cgemm": 5}
 
 
 class QtxMat(Structure):
@@ -47,6 +49,9 @@ SIGNATURES = {
     "qtx_last_error": (ctypes.c_char_p, []),
     "qtx_zgemm_batched": (c_int, [c_int, c_int, c_int, c_int64, c_double, c_double, QtxMat, c_int,
                                   QtxMat, c_int, c_double, c_double, QtxMat, c_int, QtxMat, c_void_p]),
+    "qtx_cgemm_batched": (c_int, [c_int, c_int, c_int, c_int64, ctypes.c_float, ctypes.c_float, QtxMat, c_int,
+                                  QtxMat, c_int, ctypes.c_float, ctypes.c_float, QtxMat, c_int, QtxMat, c_void_p,
+                                  c_void_p]),
     "qtx_zinv_batched": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p]),
     "qtx_selected_inv_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64]),
     "qtx_selected_inv": (c_int, [POINTER(QtxBT), POINTER(QtxMat), POINTER(QtxBT), c_int64, c_void_p,
@@ -58,10 +63,19 @@ SIGNATURES = {
                                    POINTER(QtxMat), POINTER(QtxMat), POINTER(QtxBT), POINTER(QtxBT),
                                    POINTER(QtxBT), c_void_p, QtxMat, c_void_p, c_int, c_int64,
                                    c_void_p, c_void_p, c_size_t, c_void_p]),
+    "qtx_selected_solve_mixed_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64, c_int]),
+    "qtx_selected_solve_mixed": (c_int, [POINTER(QtxBT), POINTER(QtxBT), POINTER(QtxBT), POINTER(QtxMat),
+                                         POINTER(QtxMat), POINTER(QtxMat), POINTER(QtxBT), POINTER(QtxBT),
+                                         POINTER(QtxBT), c_void_p, QtxMat, c_void_p, c_int, c_int64,
+                                         c_void_p, c_void_p, c_size_t, c_void_p]),
+    "qtx_convert": (c_int, [c_int, c_int, c_int64, QtxMat, c_int, QtxMat, c_int, c_void_p]),
     "qtx_sancho_rubio_workspace": (c_size_t, [c_int, c_int64]),
     "qtx_sancho_rubio": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, QtxMat, c_int, c_double, c_int,
                                  POINTER(c_int), POINTER(c_int), c_void_p, c_void_p, c_void_p, c_size_t,
                                  c_void_p]),
+    "qtx_sancho_rubio_multi": (c_int, [c_int, c_int, POINTER(c_int64), POINTER(QtxMat), POINTER(QtxMat),
+                                       POINTER(QtxMat), POINTER(QtxMat), c_int, c_double, c_int, POINTER(c_int),
+                                       POINTER(c_int), c_void_p, c_void_p, c_size_t, c_void_p]),
     "qtx_obc_workspace": (c_size_t, [c_int, c_int64]),
     "qtx_contact_self_energy": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, c_void_p, QtxMat, QtxMat,
                                         QtxMat, c_void_p, c_size_t, c_void_p]),

@@ -23,10 +23,16 @@ const char* get_error() { return g_error.c_str(); }
 int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_t batch, int* info,
                      Workspace& ws, cudaStream_t s);
 int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaStream_t s);
+int selected_solve_mixed_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws,
+                             cudaStream_t s);
 size_t sancho_rubio_ws(int n, int64_t batch);
 int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
                      int max_iterations, double tol, int per_energy, int* iterations,
                      int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s);
+int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_mat* aii,
+                           const qtx_mat* aij, const qtx_mat* aji, const qtx_mat* x,
+                           int max_iterations, double tol, int per_energy, int* iterations,
+                           int* converged, int* info, Workspace& ws, cudaStream_t s);
 size_t obc_refine_ws(int n, int64_t batch);
 int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x, MatRef xref,
                    double* rel, double* abs_res, int* info, Workspace& ws, cudaStream_t s);
@@ -105,15 +111,18 @@ int need_ws(void* base, size_t bytes, size_t need, const char* who) {
   return QTX_OK;
 }
 
-size_t solve_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch, int cur) {
-  // Mirrors the allocation order of selected_solve_run.
+// Workspace of a selected solve: a dry run of the driver's allocations.
+size_t solve_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch, int cur, int mixed) {
+  SolveIO io;
+  io.a.n = nb;
+  io.a.bs.assign(bs, bs + nb);
+  z64 dummy;
+  io.current = cur ? &dummy : nullptr;
   Workspace ws;
-  int bm = 0;
-  for (int i = 0; i < nb; ++i) bm = bs[i] > bm ? bs[i] : bm;
-  const int sets = 3 + (cur ? 2 : 0);
-  for (int k = 0; k < sets; ++k)
-    for (int i = 0; i < nb; ++i) ws.mat(bs[i], bs[i], batch);
-  for (int k = 0; k < 19; ++k) ws.mat(bm, bm, batch);
+  if (mixed)
+    selected_solve_mixed_run(io, batch, nullptr, ws, nullptr);
+  else
+    selected_solve_run(io, batch, nullptr, ws, nullptr);
   return ws.off + 256;
 }
 
@@ -166,6 +175,35 @@ int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, doubl
   });
 }
 
+int qtx_cgemm_batched(int m, int n, int k, int64_t batch, float alpha_re, float alpha_im, qtx_mat a,
+                      int op_a, qtx_mat b, int op_b, float beta_re, float beta_im, qtx_mat d,
+                      int op_d, qtx_mat c, int* err, qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || k < 0 || batch < 0 || (op_a != 0 && op_a != 1) ||
+        (op_b != 0 && op_b != 1) || (op_d != 0 && op_d != 1) || c.ptr == nullptr) {
+      set_error("qtx_cgemm_batched: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    CGemmDesc g;
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.batch = batch;
+    g.A = from_abi(a);
+    g.B = from_abi(b);
+    g.opA = op_a;
+    g.opB = op_b;
+    g.alpha = make_float2(alpha_re, alpha_im);
+    g.C = from_abi(c);
+    g.err = err;
+    if (d.ptr != nullptr) {
+      g.add[0] = CAddend{from_abi(d), make_float2(beta_re, beta_im), op_d};
+      g.nadd = 1;
+    }
+    return cgemm_tc(g, (cudaStream_t)stream);
+  });
+}
+
 int qtx_zinv_batched(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, qtx_stream stream) {
   return guarded([&] {
     if (n < 0 || batch < 0 || a.ptr == nullptr || x.ptr == nullptr) {
@@ -205,7 +243,7 @@ int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt*
 size_t qtx_selected_solve_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch,
                                     int return_current) {
   if (num_blocks <= 0 || block_sizes == nullptr || batch <= 0) return 0;
-  return solve_ws_bytes(num_blocks, block_sizes, batch, return_current);
+  return solve_ws_bytes(num_blocks, block_sizes, batch, return_current, 0);
 }
 
 int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt* sigma_greater,
@@ -226,7 +264,7 @@ int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt
     QTX_TRY(check_bt(xl, "xl", N, a->block_sizes));
     QTX_TRY(check_bt(xg, "xg", N, a->block_sizes));
     QTX_TRY(check_bt(xr, "xr", N, a->block_sizes));
-    const size_t need = solve_ws_bytes(N, a->block_sizes, batch, current != nullptr);
+    const size_t need = solve_ws_bytes(N, a->block_sizes, batch, current != nullptr, 0);
     QTX_TRY(need_ws(workspace, workspace_bytes, need, "qtx_selected_solve"));
     cudaStream_t s = (cudaStream_t)stream;
     if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
@@ -253,6 +291,79 @@ int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt
   });
 }
 
+size_t qtx_selected_solve_mixed_workspace(int32_t num_blocks, const int32_t* block_sizes,
+                                          int64_t batch, int return_current) {
+  if (num_blocks <= 0 || block_sizes == nullptr || batch <= 0) return 0;
+  return solve_ws_bytes(num_blocks, block_sizes, batch, return_current, 1);
+}
+
+int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
+                             const qtx_bt* sigma_greater, const qtx_mat* obc_retarded,
+                             const qtx_mat* obc_lesser, const qtx_mat* obc_greater, const qtx_bt* xl,
+                             const qtx_bt* xg, const qtx_bt* xr, void* current, qtx_mat g0n,
+                             double* density, int flags, int64_t batch, int* info, void* workspace,
+                             size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (a == nullptr || batch <= 0) {
+      set_error("qtx_selected_solve_mixed: null system matrix or empty batch");
+      return (int)QTX_ERR_ARG;
+    }
+    QTX_TRY(check_bt(a, "a", 0, nullptr));
+    const int N = a->num_blocks;
+    QTX_TRY(check_bt(sigma_lesser, "sigma_lesser", N, a->block_sizes));
+    QTX_TRY(check_bt(sigma_greater, "sigma_greater", N, a->block_sizes));
+    QTX_TRY(check_bt(xl, "xl", N, a->block_sizes));
+    QTX_TRY(check_bt(xg, "xg", N, a->block_sizes));
+    QTX_TRY(check_bt(xr, "xr", N, a->block_sizes));
+    const size_t need = solve_ws_bytes(N, a->block_sizes, batch, current != nullptr, 1);
+    QTX_TRY(need_ws(workspace, workspace_bytes, need, "qtx_selected_solve_mixed"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+    if (current)
+      QTX_CHECK_CUDA(cudaMemsetAsync(current, 0, sizeof(z64) * batch * (N + 1), s));
+    SolveIO io;
+    io.a = bt_from_abi(a);
+    io.sl = bt_from_abi(sigma_lesser);
+    io.sg = bt_from_abi(sigma_greater);
+    io.xl = bt_from_abi(xl);
+    io.xg = bt_from_abi(xg);
+    io.xr = bt_from_abi(xr);
+    std::vector<MatRef> orr = obc_vec(obc_retarded, N), ol = obc_vec(obc_lesser, N),
+                        og = obc_vec(obc_greater, N);
+    io.obc_r = orr.empty() ? nullptr : orr.data();
+    io.obc_l = ol.empty() ? nullptr : ol.data();
+    io.obc_g = og.empty() ? nullptr : og.data();
+    io.current = static_cast<z64*>(current);
+    io.g0n = from_abi(g0n);
+    io.density = density;
+    io.symmetric = (flags & QTX_SOLVE_SYMMETRIC_OUT) ? 1 : 0;
+    Workspace ws = bind(workspace, workspace_bytes);
+    return selected_solve_mixed_run(io, batch, info, ws, s);
+  });
+}
+
+int qtx_convert(int m, int n, int64_t batch, qtx_mat in, int in_dtype, qtx_mat out, int out_dtype,
+                qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || batch < 0 || in.ptr == nullptr || out.ptr == nullptr) {
+      set_error("qtx_convert: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (in_dtype == QTX_C64 && out_dtype == QTX_C128)
+      return convert_c64_to_c128(m, n, batch, from_abi(in), from_abi(out), s);
+    if (in_dtype == QTX_C128 && out_dtype == QTX_C64)
+      return convert_c128_to_c64(m, n, batch, from_abi(in), from_abi(out), s);
+    Addend t{from_abi(in), make_double2(1.0, 0.0), 0};
+    if (in_dtype == QTX_C128 && out_dtype == QTX_C128)
+      return zcombine(m, n, batch, from_abi(out), &t, 1, nullptr, s);
+    if (in_dtype == QTX_C64 && out_dtype == QTX_C64)
+      return ccombine(m, n, batch, from_abi(out), &t, 1, nullptr, s);
+    set_error("qtx_convert: unknown dtype");
+    return (int)QTX_ERR_ARG;
+  });
+}
+
 size_t qtx_sancho_rubio_workspace(int n, int64_t batch) {
   if (n <= 0 || batch <= 0) return 0;
   return sancho_rubio_ws(n, batch);
@@ -275,6 +386,34 @@ int qtx_sancho_rubio(int n, int64_t batch, qtx_mat a_ii, qtx_mat a_ij, qtx_mat a
     return sancho_rubio_run(n, batch, from_abi(a_ii), from_abi(a_ij), from_abi(a_ji), from_abi(x),
                             max_iterations, tol, per_energy, iterations, converged, delta_out, info,
                             ws, s);
+  });
+}
+
+int qtx_sancho_rubio_multi(int n, int num_systems, const int64_t* batches, const qtx_mat* a_ii,
+                           const qtx_mat* a_ij, const qtx_mat* a_ji, const qtx_mat* x,
+                           int max_iterations, double tol, int per_energy, int* iterations,
+                           int* converged, int* info, void* workspace, size_t workspace_bytes,
+                           qtx_stream stream) {
+  return guarded([&] {
+    if (n <= 0 || n > 1024 || num_systems <= 0 || batches == nullptr || a_ii == nullptr ||
+        a_ij == nullptr || a_ji == nullptr || x == nullptr || max_iterations < 0) {
+      set_error("qtx_sancho_rubio_multi: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    int64_t total = 0;
+    for (int k = 0; k < num_systems; ++k) {
+      if (batches[k] <= 0 || a_ii[k].ptr == nullptr || x[k].ptr == nullptr) {
+        set_error("qtx_sancho_rubio_multi: empty system or null matrix");
+        return (int)QTX_ERR_ARG;
+      }
+      total += batches[k];
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, sancho_rubio_ws(n, total), "qtx_sancho_rubio_multi"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * total, s));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return sancho_rubio_multi_run(n, num_systems, batches, a_ii, a_ij, a_ji, x, max_iterations, tol,
+                                  per_energy, iterations, converged, info, ws, s);
   });
 }
 

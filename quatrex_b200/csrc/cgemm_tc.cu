@@ -1,0 +1,466 @@
+// Batched complex64 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a)
+// with split-TF32 products accumulated in FP32 (the mixed-precision path).
+//
+//   out = alpha op(A) op(B) + sum_t coef_t op_t(D_t)     (complex64 in / out)
+//
+// Each FP32 operand x is split into x_hi = tf32(x) and x_lo = tf32(x - x_hi);
+// a real product is a_hi b_hi + a_hi b_lo + a_lo b_hi (the lo*lo term is
+// below FP32 rounding). A complex product is the 4M combination of real
+// products, with the subtraction folded into the instruction descriptor's
+// negate bit: 12 tcgen05.mma.kind::tf32 per K step of 8.
+//
+// CTA tile 128 x 64 (one UMMA M=128, N=64), K block 32 FP32 (128-byte rows,
+// SWIZZLE_128B K-major), two shared-memory stages. All four warps stage the
+// next K block (global complex64 -> split planes, swizzled, into the free
+// stage) while the single issuing thread's MMAs for the current block run
+// asynchronously; completion is tracked with tcgen05.commit on one mbarrier
+// per stage. Accumulators live in TMEM (Re in columns 0-63, Im in 64-127)
+// and are read back with tcgen05.ld for the fused epilogue. Every mbarrier
+// wait is bounded; on a time-out the CTA raises the error flag, skips its
+// epilogue, frees its TMEM and returns.
+#include "common.cuh"
+
+namespace qtx {
+namespace {
+
+constexpr int TM = 128;       // UMMA M
+constexpr int TN = 64;        // UMMA N
+constexpr int TK = 32;        // fp32 elements per K block (128 B rows)
+constexpr int THREADS = 128;  // four warps
+constexpr int PLANE_A = TM * TK * 4;  // bytes of one A plane (16 KB)
+constexpr int PLANE_B = TN * TK * 4;  // bytes of one B plane (8 KB)
+constexpr int STAGE_BYTES = 4 * PLANE_A + 4 * PLANE_B;  // re/im x hi/lo for A and B
+constexpr int STAGES = 2;
+constexpr int TMEM_COLS = 128;
+constexpr long long kWaitLimit = 1ll << 26;  // bounded mbarrier polls
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ float tf32_trunc(float x) {
+  return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+}
+
+// Byte offset of the 16-byte chunk holding (row, k4-chunk) in a SWIZZLE_128B
+// K-major tile: 8-row groups of 1024 B, chunk index XOR (row % 8).
+__device__ __forceinline__ uint32_t sw128_offset(int row, int chunk) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
+}
+
+// UMMA shared-memory descriptor, K-major SWIZZLE_128B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)(1) << 16;             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;     // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;               // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;               // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32, K-major both, N = 64, M = 128.
+__host__ __device__ constexpr uint32_t make_idesc(bool neg_a) {
+  return (1u << 4)                  // D format f32
+         | (2u << 7)                // A tf32
+         | (2u << 10)               // B tf32
+         | ((neg_a ? 1u : 0u) << 13)
+         | ((uint32_t)(TN >> 3) << 17)
+         | ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity));
+  return ok != 0;
+}
+
+// Bounded wait; returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+      smem_addr(bar)));
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::);
+}
+
+struct Args {
+  int M, N, K;
+  int64_t batch;
+  MatRef A, B;
+  int opA, opB;
+  float2 alpha;
+  struct Add {
+    MatRef m;
+    float2 coef;
+    int ct;
+  } add[kMaxAddends];
+  int nadd, nadd3;
+  MatRef C, C2, C3;
+  float2 coef2, scale3;
+  int* err;
+};
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Stage one K block: op(A) rows [m0, m0+128) x k [k0, k0+32) into the four A
+// planes and op(B) columns [n0, n0+64) x k into the four B planes.
+template <int OPA, int OPB>
+__device__ __forceinline__ void stage_block(const Args& a, const c32* Ag, const c32* Bg, uint8_t* st,
+                                            int m0, int n0, int k0, int tid) {
+  uint8_t* ar_h = st;
+  uint8_t* ar_l = st + PLANE_A;
+  uint8_t* ai_h = st + 2 * PLANE_A;
+  uint8_t* ai_l = st + 3 * PLANE_A;
+  uint8_t* bp = st + 4 * PLANE_A;
+  uint8_t* br_h = bp;
+  uint8_t* br_l = bp + PLANE_B;
+  uint8_t* bi_h = bp + 2 * PLANE_B;
+  uint8_t* bi_l = bp + 3 * PLANE_B;
+  // A: 128 rows x 8 chunks of 4 k values; 1024 tasks over 128 threads.
+#pragma unroll 2
+  for (int t = tid; t < TM * (TK / 4); t += THREADS) {
+    int row, chunk;
+    if (OPA == 0) {  // k contiguous in memory: lanes walk the chunks of a row
+      row = t >> 3;
+      chunk = t & 7;
+    } else {  // row index contiguous in memory: lanes walk rows
+      row = t & (TM - 1);
+      chunk = t >> 7;
+    }
+    float4 hr, lr, hi, li;
+    float* phr = &hr.x;
+    float* plr = &lr.x;
+    float* phi = &hi.x;
+    float* pli = &li.x;
+    const int gr = m0 + row;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = k0 + chunk * 4 + e;
+      float2 v = make_float2(0.f, 0.f);
+      if (gr < a.M && gk < a.K) {
+        if (OPA == 0) {
+          v = Ag[(int64_t)gr * a.A.ld + gk];
+        } else {
+          v = Ag[(int64_t)gk * a.A.ld + gr];
+          v.y = -v.y;
+        }
+      }
+      const float rh = tf32_trunc(v.x), ih = tf32_trunc(v.y);
+      phr[e] = rh;
+      plr[e] = tf32_trunc(v.x - rh);
+      phi[e] = ih;
+      pli[e] = tf32_trunc(v.y - ih);
+    }
+    const uint32_t off = sw128_offset(row, chunk);
+    *reinterpret_cast<float4*>(ar_h + off) = hr;
+    *reinterpret_cast<float4*>(ar_l + off) = lr;
+    *reinterpret_cast<float4*>(ai_h + off) = hi;
+    *reinterpret_cast<float4*>(ai_l + off) = li;
+  }
+  // B: 64 rows (columns of op(B)) x 8 chunks; 512 tasks.
+#pragma unroll 2
+  for (int t = tid; t < TN * (TK / 4); t += THREADS) {
+    int row, chunk;
+    if (OPB == 1) {  // op(B)[k][n] = conj(B[n][k]): k contiguous
+      row = t >> 3;
+      chunk = t & 7;
+    } else {  // B[k][n]: n contiguous, lanes walk n
+      row = t & (TN - 1);
+      chunk = t >> 6;
+    }
+    float4 hr, lr, hi, li;
+    float* phr = &hr.x;
+    float* plr = &lr.x;
+    float* phi = &hi.x;
+    float* pli = &li.x;
+    const int gn = n0 + row;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = k0 + chunk * 4 + e;
+      float2 v = make_float2(0.f, 0.f);
+      if (gn < a.N && gk < a.K) {
+        if (OPB == 0) {
+          v = Bg[(int64_t)gk * a.B.ld + gn];
+        } else {
+          v = Bg[(int64_t)gn * a.B.ld + gk];
+          v.y = -v.y;
+        }
+      }
+      const float rh = tf32_trunc(v.x), ih = tf32_trunc(v.y);
+      phr[e] = rh;
+      plr[e] = tf32_trunc(v.x - rh);
+      phi[e] = ih;
+      pli[e] = tf32_trunc(v.y - ih);
+    }
+    const uint32_t off = sw128_offset(row, chunk);
+    *reinterpret_cast<float4*>(br_h + off) = hr;
+    *reinterpret_cast<float4*>(br_l + off) = lr;
+    *reinterpret_cast<float4*>(bi_h + off) = hi;
+    *reinterpret_cast<float4*>(bi_l + off) = li;
+  }
+}
+
+// The 12 MMAs of one K step (8 fp32) on stage base addresses.
+__device__ __forceinline__ void issue_kstep(uint32_t tmem, uint32_t sa, uint32_t sb, int kk,
+                                            bool first) {
+  const uint32_t koff = (uint32_t)kk * 32;  // bytes along the 128-byte row
+  const uint64_t arh = make_desc(sa + 0 * PLANE_A + koff), arl = make_desc(sa + 1 * PLANE_A + koff);
+  const uint64_t aih = make_desc(sa + 2 * PLANE_A + koff), ail = make_desc(sa + 3 * PLANE_A + koff);
+  const uint64_t brh = make_desc(sb + 0 * PLANE_B + koff), brl = make_desc(sb + 1 * PLANE_B + koff);
+  const uint64_t bih = make_desc(sb + 2 * PLANE_B + koff), bil = make_desc(sb + 3 * PLANE_B + koff);
+  constexpr uint32_t ID = make_idesc(false), IDN = make_idesc(true);
+  const uint32_t re = tmem, im = tmem + TN;
+  // Re += Ar Br - Ai Bi  (small terms first)
+  mma_tf32(re, arl, brh, ID, first ? 0u : 1u);
+  mma_tf32(re, arh, brl, ID, 1u);
+  mma_tf32(re, arh, brh, ID, 1u);
+  mma_tf32(re, ail, bih, IDN, 1u);
+  mma_tf32(re, aih, bil, IDN, 1u);
+  mma_tf32(re, aih, bih, IDN, 1u);
+  // Im += Ar Bi + Ai Br
+  mma_tf32(im, arl, bih, ID, first ? 0u : 1u);
+  mma_tf32(im, arh, bil, ID, 1u);
+  mma_tf32(im, arh, bih, ID, 1u);
+  mma_tf32(im, ail, brh, ID, 1u);
+  mma_tf32(im, aih, brl, ID, 1u);
+  mma_tf32(im, aih, brh, ID, 1u);
+}
+
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte alignment for the SWIZZLE_128B atoms.
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* stages = smem;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + STAGES);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int m0 = blockIdx.y * TM;
+  const int n0 = blockIdx.x * TN;
+  const int KB = (a.K + TK - 1) / TK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  uint32_t phase[STAGES] = {0, 0};
+  bool ok = true;
+
+  for (int64_t b = blockIdx.z; b < a.batch && ok; b += gridDim.z) {
+    const c32* Ag = at<const c32>(a.A, b);
+    const c32* Bg = at<const c32>(a.B, b);
+    if (KB > 0) {
+      stage_block<OPA, OPB>(a, Ag, Bg, stages, m0, n0, 0, tid);
+      fence_async_smem();
+      __syncthreads();
+    }
+    for (int kb = 0; kb < KB; ++kb) {
+      const int s = kb % STAGES;
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        const uint32_t sa = smem_addr(stages + s * STAGE_BYTES);
+        const uint32_t sb = sa + 4 * PLANE_A;
+#pragma unroll
+        for (int kk = 0; kk < TK / 8; ++kk) issue_kstep(tmem, sa, sb, kk, kb == 0 && kk == 0);
+        mma_commit(&bars[s]);
+      }
+      if (kb + 1 < KB) {
+        const int s1 = (kb + 1) % STAGES;
+        // The stage being refilled was read by the MMAs of block kb - 1.
+        if (kb >= 1) {
+          if (!mbar_wait(&bars[s1], phase[s1])) ok = false;
+          phase[s1] ^= 1u;
+        }
+        if (ok) stage_block<OPA, OPB>(a, Ag, Bg, stages + s1 * STAGE_BYTES, m0, n0, (kb + 1) * TK, tid);
+        fence_async_smem();
+      }
+      __syncthreads();
+      if (!__syncthreads_and(ok)) {
+        ok = false;
+        break;
+      }
+    }
+    // Wait for the last block's MMAs (and the one before, if not yet waited).
+    if (KB > 0 && ok) {
+      const int sl = (KB - 1) % STAGES;
+      if (KB >= 2) {
+        const int sp = (KB - 2) % STAGES;
+        if (!mbar_wait(&bars[sp], phase[sp])) ok = false;
+        phase[sp] ^= 1u;
+      }
+      if (!mbar_wait(&bars[sl], phase[sl])) ok = false;
+      phase[sl] ^= 1u;
+    }
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+
+    // Epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows.
+    const int r = m0 + warp * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int c0 = 0; c0 < TN; c0 += 16) {
+      uint32_t vr[16], vi[16];
+      if (KB > 0) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+            : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]),
+              "=r"(vr[6]), "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]),
+              "=r"(vr[12]), "=r"(vr[13]), "=r"(vr[14]), "=r"(vr[15])
+            : "r"(lane_base + (uint32_t)c0));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+            : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]),
+              "=r"(vi[6]), "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]),
+              "=r"(vi[12]), "=r"(vi[13]), "=r"(vi[14]), "=r"(vi[15])
+            : "r"(lane_base + (uint32_t)(TN + c0)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0u;
+      }
+      if (r < a.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = n0 + c0 + j;
+          if (c >= a.N) continue;
+          float2 v = cmulf(a.alpha, make_float2(__uint_as_float(vr[j]), __uint_as_float(vi[j])));
+          for (int t = 0; t < a.nadd; ++t) {
+            const auto& ad = a.add[t];
+            const c32* p = at<const c32>(ad.m, b);
+            float2 x = ad.ct ? p[(int64_t)c * ad.m.ld + r] : p[(int64_t)r * ad.m.ld + c];
+            if (ad.ct) x.y = -x.y;
+            const float2 y = cmulf(ad.coef, x);
+            v.x += y.x;
+            v.y += y.y;
+          }
+          if (!a.C3.null()) {
+            float2 v3 = cmulf(a.scale3, v);
+            for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) {
+              const auto& ad = a.add[t];
+              const c32* p = at<const c32>(ad.m, b);
+              float2 x = ad.ct ? p[(int64_t)c * ad.m.ld + r] : p[(int64_t)r * ad.m.ld + c];
+              if (ad.ct) x.y = -x.y;
+              const float2 y = cmulf(ad.coef, x);
+              v3.x += y.x;
+              v3.y += y.y;
+            }
+            at<c32>(a.C3, b)[(int64_t)r * a.C3.ld + c] = v3;
+          }
+          if (!a.C2.null())
+            at<c32>(a.C2, b)[(int64_t)c * a.C2.ld + r] = cmulf(a.coef2, make_float2(v.x, -v.y));
+          if (!a.C.null()) at<c32>(a.C, b)[(int64_t)r * a.C.ld + c] = v;
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+  }
+  if (!ok && tid == 0 && a.err != nullptr) atomicExch(a.err, 1);
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+template <int OPA, int OPB>
+int launch(const Args& a, cudaStream_t s) {
+  const size_t smem = (size_t)STAGES * STAGE_BYTES + 64 + 1024;
+  QTX_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<OPA, OPB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((a.N + TN - 1) / TN, (a.M + TM - 1) / TM, (unsigned)(a.batch < 65535 ? a.batch : 65535));
+  ProfScope prof(QTX_KERNEL_CGEMM, 8.0 * a.M * a.N * (double)a.K * (double)a.batch, s);
+  cgemm_tc_kernel<OPA, OPB><<<grid, THREADS, smem, s>>>(a);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+}  // namespace
+
+int cgemm_tc(const CGemmDesc& d, cudaStream_t s) {
+  if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return QTX_OK;
+  if (d.nadd < 0 || d.nadd3 < 0 || d.nadd + d.nadd3 > kMaxAddends ||
+      (d.K > 0 && (d.A.null() || d.B.null())) || (d.C.null() && d.C3.null())) {
+    set_error("cgemm_tc: invalid arguments (null operand or output, or too many addends)");
+    return QTX_ERR_ARG;
+  }
+  Args a{};
+  a.M = d.M;
+  a.N = d.N;
+  a.K = d.K;
+  a.batch = d.batch;
+  a.A = d.A;
+  a.B = d.B;
+  a.opA = d.opA;
+  a.opB = d.opB;
+  a.alpha = d.alpha;
+  a.nadd = 0;
+  a.nadd3 = 0;
+  for (int t = 0; t < d.nadd + d.nadd3; ++t) {
+    if (d.add[t].m.null()) continue;
+    const int k = a.nadd + a.nadd3;
+    a.add[k].m = d.add[t].m;
+    a.add[k].coef = d.add[t].coef;
+    a.add[k].ct = d.add[t].conj_trans;
+    if (t < d.nadd)
+      ++a.nadd;
+    else
+      ++a.nadd3;
+  }
+  a.C = d.C;
+  a.C2 = d.C2;
+  a.C3 = d.C3;
+  a.coef2 = d.coef2;
+  a.scale3 = d.scale3;
+  a.err = d.err;
+  switch (d.opA * 2 + d.opB) {
+    case 0: return launch<0, 0>(a, s);
+    case 1: return launch<0, 1>(a, s);
+    case 2: return launch<1, 0>(a, s);
+    default: return launch<1, 1>(a, s);
+  }
+}
+
+}  // namespace qtx

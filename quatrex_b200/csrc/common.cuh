@@ -110,6 +110,29 @@ struct GemmDesc {
 
 int zgemm(const GemmDesc& d, cudaStream_t s);
 
+// Complex64 GEMM on tcgen05 with split-TF32 products (cgemm_tc.cu):
+//   C = alpha op(A) op(B) + sum_t coef_t op_t(D_t);  C2 = coef2 C^H (optional).
+struct CAddend {
+  MatRef m;
+  float2 coef;
+  int conj_trans;
+};
+struct CGemmDesc {
+  int M = 0, N = 0, K = 0;
+  int64_t batch = 0;
+  MatRef A, B;
+  int opA = 0, opB = 0;
+  float2 alpha{1.f, 0.f};
+  CAddend add[kMaxAddends];
+  int nadd = 0;
+  int nadd3 = 0;  // addends of C3, stored after the primary ones
+  MatRef C, C2, C3;
+  float2 coef2{1.f, 0.f};
+  float2 scale3{1.f, 0.f};
+  int* err = nullptr;  // set to 1 if an mbarrier wait timed out
+};
+int cgemm_tc(const CGemmDesc& d, cudaStream_t s);
+
 // Batched in-place Gauss-Jordan inversion with partial pivoting (zinv.cu).
 // X <- A^{-1} for each of `batch` n x n matrices; X may alias A. `info[b]`
 // (device, optional) receives 0 or the 1-based column of a zero pivot.
@@ -120,12 +143,25 @@ int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active,
 int zcombine(int m, int n, int64_t batch, MatRef out, const Addend* terms, int nterms,
              const int* active, cudaStream_t s);
 
+// complex64 twin of zcombine (arithmetic in double).
+int ccombine(int m, int n, int64_t batch, MatRef out, const Addend* terms, int nterms,
+             const int* active, cudaStream_t s);
+
 // out = 0.5 (X - X^H); optional density[b, off + r] = Im X[r, r].
 int zantiherm(int n, int64_t batch, MatRef X, MatRef out, double* density, int64_t dens_stride,
               int64_t dens_off, cudaStream_t s);
+int cantiherm(int n, int64_t batch, MatRef X, MatRef out, double* density, int64_t dens_stride,
+              int64_t dens_off, cudaStream_t s);
+
+// Element-type conversion of an m x n stack.
+int convert_c64_to_c128(int m, int n, int64_t batch, MatRef in, MatRef out, cudaStream_t s);
+int convert_c128_to_c64(int m, int n, int64_t batch, MatRef in, MatRef out, cudaStream_t s);
 
 // result[b * rstride + roff] (+)= sign * Tr(X_b Y_b)  (complex, n x n).
 int ztrace_prod(int n, int64_t batch, MatRef X, MatRef Y, z64 coef, z64* result, int64_t rstride,
+                int64_t roff, int accumulate, cudaStream_t s);
+
+int ctrace_prod(int n, int64_t batch, MatRef X, MatRef Y, z64 coef, z64* result, int64_t rstride,
                 int64_t roff, int accumulate, cudaStream_t s);
 
 // delta[b] = || |X_b| + |Y_b| ||_F / 2   (Sancho-Rubio convergence measure).
@@ -139,6 +175,7 @@ int znorm_diff(int n, int64_t batch, MatRef X, MatRef Y, double* nrm_diff, doubl
 
 // T[b] = Re Tr(GamL G GamR G^H) given P = GamL G GamR: Re sum conj(G) .* P.
 int zre_inner(int m, int n, int64_t batch, MatRef P, MatRef G, double* out, cudaStream_t s);
+int cre_inner(int m, int n, int64_t batch, MatRef P, MatRef G, double* out, cudaStream_t s);
 
 // Launch profiler (profile.cu): RAII bracket of one kernel launch.
 class ProfScope {
@@ -167,10 +204,10 @@ struct Workspace {
     if (base && off > cap) overflow = true;
     return p;
   }
-  MatRef mat(int rows, int cols, int64_t batch) {
+  MatRef mat(int rows, int cols, int64_t batch, size_t elem = sizeof(z64)) {
     const int64_t stride = (int64_t)rows * cols;
     MatRef m;
-    m.p = take((size_t)stride * batch * sizeof(z64));
+    m.p = take((size_t)stride * batch * elem);
     m.ld = cols;
     m.stride = stride;
     return m;

@@ -152,29 +152,143 @@ int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_
 }
 
 // ---------------------------------------------------------------------------
-// selected_solve (rgf.py:115-438)
+// selected_solve (rgf.py:115-438), generic over the arithmetic:
+//   Fp64  -- complex128 blocks, DMMA products, FP64 inverses;
+//   Mixed -- complex64 blocks, tcgen05 split-TF32 products with FP32
+//            accumulation, FP64 Gauss-Jordan inverses of the Schur
+//            complements (upcast, invert, round back).
 // ---------------------------------------------------------------------------
+namespace {
 
-int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaStream_t s) {
+struct Fp64 {
+  static constexpr size_t E = sizeof(z64);
+  static constexpr bool kInvTmp = false;
+  using G = Gemm;
+  static int combine(int m, int n, int64_t b, MatRef out, const Addend* t, int nt, cudaStream_t s) {
+    return zcombine(m, n, b, out, t, nt, nullptr, s);
+  }
+  static int antiherm(int n, int64_t b, MatRef X, MatRef out, double* d, int64_t ds, int64_t doff,
+                      cudaStream_t s) {
+    return zantiherm(n, b, X, out, d, ds, doff, s);
+  }
+  static int trace(int n, int64_t b, MatRef X, MatRef Y, z64 coef, z64* r, int64_t rs, int64_t ro,
+                   int acc, cudaStream_t s) {
+    return ztrace_prod(n, b, X, Y, coef, r, rs, ro, acc, s);
+  }
+  static int inv(int n, int64_t b, MatRef X, int* info, MatRef, cudaStream_t s) {
+    return zinv(n, b, X, X, info, nullptr, s);
+  }
+};
+
+inline float2 f2(z64 v) { return make_float2((float)v.x, (float)v.y); }
+
+struct MixedGemm {
+  CGemmDesc d;
+  MixedGemm(int M, int N, int K, int64_t batch, MatRef A, int opA, MatRef B, int opB, MatRef C,
+            z64 alpha = ONE) {
+    d.M = M;
+    d.N = N;
+    d.K = K;
+    d.batch = batch;
+    d.A = A;
+    d.B = B;
+    d.opA = opA;
+    d.opB = opB;
+    d.alpha = f2(alpha);
+    d.C = C;
+  }
+  MixedGemm& plus(const MatRef& m, z64 coef, int ct = 0) {
+    if (!m.null()) d.add[d.nadd++] = CAddend{m, f2(coef), ct};
+    return *this;
+  }
+  MixedGemm& store_h(const MatRef& c2, z64 coef) {
+    d.C2 = c2;
+    d.coef2 = f2(coef);
+    return *this;
+  }
+  MixedGemm& second(const MatRef& c3, z64 scale) {
+    d.C3 = c3;
+    d.scale3 = f2(scale);
+    return *this;
+  }
+  MixedGemm& plus3(const MatRef& m, z64 coef, int ct = 0) {
+    if (!m.null()) d.add[d.nadd + d.nadd3++] = CAddend{m, f2(coef), ct};
+    return *this;
+  }
+  int run(cudaStream_t s) {
+    if (d.K > 0 && (d.A.null() || d.B.null())) {
+      // A zero operand: only the addends remain (a combine).
+      Addend t[kMaxAddends];
+      int nt = 0;
+      for (int k = 0; k < d.nadd; ++k)
+        t[nt++] = Addend{d.add[k].m, make_double2(d.add[k].coef.x, d.add[k].coef.y), d.add[k].conj_trans};
+      if (!d.C.null()) QTX_TRY(ccombine(d.M, d.N, d.batch, d.C, t, nt, nullptr, s));
+      if (!d.C3.null() || !d.C2.null()) {
+        set_error("mixed gemm: zero operand with a second output is not supported");
+        return QTX_ERR_UNSUPPORTED;
+      }
+      return QTX_OK;
+    }
+    return cgemm_tc(d, s);
+  }
+};
+
+struct Mixed {
+  static constexpr size_t E = sizeof(c32);
+  static constexpr bool kInvTmp = true;
+  using G = MixedGemm;
+  static int combine(int m, int n, int64_t b, MatRef out, const Addend* t, int nt, cudaStream_t s) {
+    return ccombine(m, n, b, out, t, nt, nullptr, s);
+  }
+  static int antiherm(int n, int64_t b, MatRef X, MatRef out, double* d, int64_t ds, int64_t doff,
+                      cudaStream_t s) {
+    return cantiherm(n, b, X, out, d, ds, doff, s);
+  }
+  static int trace(int n, int64_t b, MatRef X, MatRef Y, z64 coef, z64* r, int64_t rs, int64_t ro,
+                   int acc, cudaStream_t s) {
+    return ctrace_prod(n, b, X, Y, coef, r, rs, ro, acc, s);
+  }
+  // The Schur complement is inverted in FP64: upcast, Gauss-Jordan, round back.
+  static int inv(int n, int64_t b, MatRef X, int* info, MatRef tmp, cudaStream_t s) {
+    MatRef t = shaped(tmp, n);
+    QTX_TRY(convert_c64_to_c128(n, n, b, X, t, s));
+    QTX_TRY(zinv(n, b, t, t, info, nullptr, s));
+    return convert_c128_to_c64(n, n, b, t, X, s);
+  }
+};
+
+template <class P>
+int copy_block_t(int m, int n, int64_t batch, MatRef dst, MatRef src, cudaStream_t s) {
+  if (dst.null()) return QTX_OK;
+  Addend t = add(src, ONE);
+  return P::combine(m, n, batch, dst, &t, 1, s);
+}
+
+}  // namespace
+
+template <class Prec>
+int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaStream_t s) {
+  using Gemm = typename Prec::G;
   const BTRef& a = io.a;
   const int N = a.n;
   const std::vector<int>& bs = a.bs;
   const int bm = max_block(bs);
   const bool want_current = io.current != nullptr;
   std::vector<MatRef> gR(N), gX[2], st[2];
-  for (int i = 0; i < N; ++i) gR[i] = ws.mat(bs[i], bs[i], batch);
+  for (int i = 0; i < N; ++i) gR[i] = ws.mat(bs[i], bs[i], batch, Prec::E);
   for (int x = 0; x < 2; ++x) {
     gX[x].resize(N);
-    for (int i = 0; i < N; ++i) gX[x][i] = ws.mat(bs[i], bs[i], batch);
+    for (int i = 0; i < N; ++i) gX[x][i] = ws.mat(bs[i], bs[i], batch, Prec::E);
   }
   if (want_current)
     for (int x = 0; x < 2; ++x) {
       st[x].resize(N);
-      for (int i = 0; i < N; ++i) st[x][i] = ws.mat(bs[i], bs[i], batch);
+      for (int i = 0; i < N; ++i) st[x][i] = ws.mat(bs[i], bs[i], batch, Prec::E);
     }
   enum { P_, M_, T_, Q_, T2_, U_, V_, W_, Z_, R1_, TT_, T1X_, T2X_, Y_, XIJ_, GA_, GB_, CA_, CB_, NT_ };
   MatRef tmp[NT_];
-  for (int k = 0; k < NT_; ++k) tmp[k] = ws.mat(bm, bm, batch);
+  for (int k = 0; k < NT_; ++k) tmp[k] = ws.mat(bm, bm, batch, Prec::E);
+  MatRef inv_tmp = Prec::kInvTmp ? ws.mat(bm, bm, batch, sizeof(z64)) : MatRef{};
   if (ws.base == nullptr) return QTX_OK;
   if (ws.overflow) {
     set_error("selected_solve: workspace too small");
@@ -198,12 +312,12 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
   // First layer (rgf.py:214-238).
   {
     Addend t[2] = {add(a.diag[0], ONE), add(obc(io.obc_r, 0), MONE)};
-    QTX_TRY(zcombine(bs[0], bs[0], batch, gR[0], t, 2, nullptr, s));
-    QTX_TRY(zinv(bs[0], batch, gR[0], gR[0], info, nullptr, s));
+    QTX_TRY(Prec::combine(bs[0], bs[0], batch, gR[0], t, 2, s));
+    QTX_TRY(Prec::inv(bs[0], batch, gR[0], info, inv_tmp, s));
     for (int x = 0; x < 2; ++x) {
       MatRef M = shaped(tmp[M_], bs[0]);
       Addend u[2] = {add(sdiag(x, 0), ONE), add(obc(obx[x], 0), ONE)};
-      QTX_TRY(zcombine(bs[0], bs[0], batch, M, u, 2, nullptr, s));
+      QTX_TRY(Prec::combine(bs[0], bs[0], batch, M, u, 2, s));
       MatRef T2 = shaped(tmp[T2_], bs[0]);
       QTX_TRY(Gemm(bs[0], bs[0], bs[0], batch, gR[0], 0, M, 0, T2).run(s));
       QTX_TRY(Gemm(bs[0], bs[0], bs[0], batch, T2, 0, gR[0], 1, gX[x][0]).run(s));
@@ -218,7 +332,7 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
                 .plus(a.diag[j], ONE)
                 .plus(obc(io.obc_r, j), MONE)
                 .run(s));
-    QTX_TRY(zinv(bs[j], batch, gR[j], gR[j], info, nullptr, s));
+    QTX_TRY(Prec::inv(bs[j], batch, gR[j], info, inv_tmp, s));
     for (int x = 0; x < 2; ++x) {
       MatRef Q{};
       if (!supper(x, i).null()) {
@@ -252,9 +366,9 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
   }
   // Last diagonal blocks (rgf.py:305-312).
   for (int x = 0; x < 2; ++x)
-    QTX_TRY(zantiherm(bs[N - 1], batch, gX[x][N - 1], odiag(x, N - 1),
+    QTX_TRY(Prec::antiherm(bs[N - 1], batch, gX[x][N - 1], odiag(x, N - 1),
                       x == 0 ? io.density : nullptr, dens_stride, offs[N - 1], s));
-  if (io.xr.n) QTX_TRY(copy_block(bs[N - 1], bs[N - 1], batch, io.xr.diag[N - 1], gR[N - 1], s));
+  if (io.xr.n) QTX_TRY(copy_block_t<Prec>(bs[N - 1], bs[N - 1], batch, io.xr.diag[N - 1], gR[N - 1], s));
 
   // Backward sweep (rgf.py:315-412).
   MatRef GRj = gR[N - 1];
@@ -304,13 +418,13 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
                   .plus(t1, ONE)
                   .plus(t1, MONE, 1)
                   .run(s));
-      QTX_TRY(zantiherm(bs[i], batch, gX[x][i], odiag(x, i), x == 0 ? io.density : nullptr,
+      QTX_TRY(Prec::antiherm(bs[i], batch, gX[x][i], odiag(x, i), x == 0 ? io.density : nullptr,
                         dens_stride, offs[i], s));
     }
     if (want_current) {
       // I_j = Tr(Sigma~^>_j X^<_jj - X^>_jj Sigma~^<_j)  (rgf.py:403-408).
-      QTX_TRY(ztrace_prod(bs[j], batch, st[1][j], gX[0][j], ONE, io.current, cur_stride, j, 0, s));
-      QTX_TRY(ztrace_prod(bs[j], batch, gX[1][j], st[0][j], MONE, io.current, cur_stride, j, 1, s));
+      QTX_TRY(Prec::trace(bs[j], batch, st[1][j], gX[0][j], ONE, io.current, cur_stride, j, 0, s));
+      QTX_TRY(Prec::trace(bs[j], batch, gX[1][j], st[0][j], MONE, io.current, cur_stride, j, 1, s));
     }
     if (want_g0n) {
       MatRef nc = shaped(tmp[(i & 1) ? CA_ : CB_], bs[N - 1]);
@@ -323,7 +437,7 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
     QTX_TRY(Gemm(bs[i], bs[i], bs[i], batch, Z, 0, gR[i], 0, Gi).plus(gR[i], ONE).run(s));
     GRj = Gi;
   }
-  if (want_g0n && N == 1) QTX_TRY(copy_block(bs[0], bs[0], batch, io.g0n, gR[0], s));
+  if (want_g0n && N == 1) QTX_TRY(copy_block_t<Prec>(bs[0], bs[0], batch, io.g0n, gR[0], s));
   if (want_current) {
     // Boundary currents (rgf.py:414-428).
     const MatRef l0 = obc(io.obc_l, 0), g0 = obc(io.obc_g, 0);
@@ -331,16 +445,25 @@ int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& w
     // Slots 0 and N start from the caller's zero initialisation; a missing
     // OBC block contributes nothing.
     if (!g0.null())
-      QTX_TRY(ztrace_prod(bs[0], batch, g0, gX[0][0], ONE, io.current, cur_stride, 0, 0, s));
+      QTX_TRY(Prec::trace(bs[0], batch, g0, gX[0][0], ONE, io.current, cur_stride, 0, 0, s));
     if (!l0.null())
-      QTX_TRY(ztrace_prod(bs[0], batch, gX[1][0], l0, MONE, io.current, cur_stride, 0, g0.null() ? 0 : 1, s));
+      QTX_TRY(Prec::trace(bs[0], batch, gX[1][0], l0, MONE, io.current, cur_stride, 0, g0.null() ? 0 : 1, s));
     if (!gn.null())
-      QTX_TRY(ztrace_prod(bs[N - 1], batch, gn, gX[0][N - 1], MONE, io.current, cur_stride, N, 0, s));
+      QTX_TRY(Prec::trace(bs[N - 1], batch, gn, gX[0][N - 1], MONE, io.current, cur_stride, N, 0, s));
     if (!ln.null())
-      QTX_TRY(ztrace_prod(bs[N - 1], batch, gX[1][N - 1], ln, ONE, io.current, cur_stride, N,
+      QTX_TRY(Prec::trace(bs[N - 1], batch, gX[1][N - 1], ln, ONE, io.current, cur_stride, N,
                           gn.null() ? 0 : 1, s));
   }
   return QTX_OK;
+}
+
+int selected_solve_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaStream_t s) {
+  return solve_impl<Fp64>(io, batch, info, ws, s);
+}
+
+int selected_solve_mixed_run(const SolveIO& io, int64_t batch, int* info, Workspace& ws,
+                             cudaStream_t s) {
+  return solve_impl<Mixed>(io, batch, info, ws, s);
 }
 
 }  // namespace qtx

@@ -109,49 +109,81 @@ size_t sancho_rubio_ws(int n, int64_t batch) {
   return ws.off + 256;
 }
 
-int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
-                     int max_iterations, double tol, int per_energy, int* iterations,
-                     int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s) {
-  MatRef eps = ws.mat(n, n, batch), eps_s = ws.mat(n, n, batch);
-  MatRef alpha[2] = {ws.mat(n, n, batch), ws.mat(n, n, batch)};
-  MatRef beta[2] = {ws.mat(n, n, batch), ws.mat(n, n, batch)};
-  MatRef inv_e = ws.mat(n, n, batch), aI = ws.mat(n, n, batch), bI = ws.mat(n, n, batch);
-  MatRef t1 = ws.mat(n, n, batch);
-  double* delta = static_cast<double*>(ws.take(sizeof(double) * batch));
-  int* active = static_cast<int*>(ws.take(sizeof(int) * batch));
-  if (ws.overflow) {
-    set_error("sancho_rubio: workspace too small");
-    return QTX_ERR_WORKSPACE;
-  }
-  {
-    Addend t = Addend{aii, ONE, 0};
-    QTX_TRY(zcombine(n, n, batch, eps, &t, 1, nullptr, s));
-    QTX_TRY(zcombine(n, n, batch, eps_s, &t, 1, nullptr, s));
-    Addend u = Addend{aji, ONE, 0};
-    QTX_TRY(zcombine(n, n, batch, alpha[0], &u, 1, nullptr, s));
-    Addend v = Addend{aij, ONE, 0};
-    QTX_TRY(zcombine(n, n, batch, beta[0], &v, 1, nullptr, s));
-  }
-  QTX_TRY(fill_int(active, batch, 1, s));
+namespace {
+
+struct SRState {
+  MatRef eps, eps_s, alpha[2], beta[2], inv_e, aI, bI, t1;
+  double* delta;
+  int* active;
+};
+
+SRState sr_state(int n, int64_t batch, Workspace& ws) {
+  SRState st;
+  st.eps = ws.mat(n, n, batch);
+  st.eps_s = ws.mat(n, n, batch);
+  st.alpha[0] = ws.mat(n, n, batch);
+  st.alpha[1] = ws.mat(n, n, batch);
+  st.beta[0] = ws.mat(n, n, batch);
+  st.beta[1] = ws.mat(n, n, batch);
+  st.inv_e = ws.mat(n, n, batch);
+  st.aI = ws.mat(n, n, batch);
+  st.bI = ws.mat(n, n, batch);
+  st.t1 = ws.mat(n, n, batch);
+  st.delta = static_cast<double*>(ws.take(sizeof(double) * batch));
+  st.active = static_cast<int*>(ws.take(sizeof(int) * batch));
+  return st;
+}
+
+MatRef offset(const MatRef& m, int64_t entries) {
+  MatRef r = m;
+  r.p = static_cast<z64*>(m.p) + entries * m.stride;
+  return r;
+}
+
+// Copies one system's inputs into entries [off, off + batch) of the state.
+int sr_load(int n, int64_t batch, int64_t off, const SRState& st, MatRef aii, MatRef aij,
+            MatRef aji, cudaStream_t s) {
+  Addend t{aii, ONE, 0};
+  QTX_TRY(zcombine(n, n, batch, offset(st.eps, off), &t, 1, nullptr, s));
+  QTX_TRY(zcombine(n, n, batch, offset(st.eps_s, off), &t, 1, nullptr, s));
+  Addend u{aji, ONE, 0};
+  QTX_TRY(zcombine(n, n, batch, offset(st.alpha[0], off), &u, 1, nullptr, s));
+  Addend v{aij, ONE, 0};
+  QTX_TRY(zcombine(n, n, batch, offset(st.beta[0], off), &v, 1, nullptr, s));
+  return QTX_OK;
+}
+
+// The decimation loop on the whole state; eps_s holds the result.
+int sr_iterate(int n, int64_t batch, const SRState& st, int max_iterations, double tol,
+               int per_energy, int* iterations, int* converged, int* info, cudaStream_t s) {
+  QTX_TRY(fill_int(st.active, batch, 1, s));
   std::vector<double> hdelta(batch);
   std::vector<int> hactive(batch, 1);
   int it = 0, cur = 0;
   bool done = false;
-  const int* mask = per_energy ? active : nullptr;
+  const int* mask = per_energy ? st.active : nullptr;
   while (it < max_iterations && !done) {
     const int nx = cur ^ 1;
-    QTX_TRY(zinv(n, batch, eps, inv_e, info, mask, s));
-    QTX_TRY(G(n, n, n, batch, alpha[cur], inv_e, aI).mask(mask).run(s));
-    QTX_TRY(G(n, n, n, batch, beta[cur], inv_e, bI).mask(mask).run(s));
+    QTX_TRY(zinv(n, batch, st.eps, st.inv_e, info, mask, s));
+    QTX_TRY(G(n, n, n, batch, st.alpha[cur], st.inv_e, st.aI).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.beta[cur], st.inv_e, st.bI).mask(mask).run(s));
     // t1 = alpha inv beta;  eps_s <- eps_s - t1.
-    QTX_TRY(G(n, n, n, batch, aI, beta[cur], t1).second(eps_s, MONE).plus3(eps_s, ONE).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.aI, st.beta[cur], st.t1)
+                .second(st.eps_s, MONE)
+                .plus3(st.eps_s, ONE)
+                .mask(mask)
+                .run(s));
     // eps <- eps - t1 - beta inv alpha.
-    QTX_TRY(G(n, n, n, batch, bI, alpha[cur], eps, MONE).plus(eps, ONE).plus(t1, MONE).mask(mask).run(s));
-    QTX_TRY(G(n, n, n, batch, aI, alpha[cur], alpha[nx]).mask(mask).run(s));
-    QTX_TRY(G(n, n, n, batch, bI, beta[cur], beta[nx]).mask(mask).run(s));
-    QTX_TRY(sr_delta(n, batch, alpha[nx], beta[nx], delta, mask, s));
+    QTX_TRY(G(n, n, n, batch, st.bI, st.alpha[cur], st.eps, MONE)
+                .plus(st.eps, ONE)
+                .plus(st.t1, MONE)
+                .mask(mask)
+                .run(s));
+    QTX_TRY(G(n, n, n, batch, st.aI, st.alpha[cur], st.alpha[nx]).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.bI, st.beta[cur], st.beta[nx]).mask(mask).run(s));
+    QTX_TRY(sr_delta(n, batch, st.alpha[nx], st.beta[nx], st.delta, mask, s));
     ++it;
-    QTX_CHECK_CUDA(cudaMemcpyAsync(hdelta.data(), delta, sizeof(double) * batch,
+    QTX_CHECK_CUDA(cudaMemcpyAsync(hdelta.data(), st.delta, sizeof(double) * batch,
                                    cudaMemcpyDeviceToHost, s));
     QTX_CHECK_CUDA(cudaStreamSynchronize(s));
     cur = nx;
@@ -168,9 +200,11 @@ int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, M
         }
       }
       if (remaining == 0) done = true;
-      if (changed && !done)
-        QTX_CHECK_CUDA(cudaMemcpyAsync(active, hactive.data(), sizeof(int) * batch,
+      if (changed && !done) {
+        QTX_CHECK_CUDA(cudaMemcpyAsync(st.active, hactive.data(), sizeof(int) * batch,
                                        cudaMemcpyHostToDevice, s));
+        QTX_CHECK_CUDA(cudaStreamSynchronize(s));
+      }
     } else {
       double mx = 0.0;
       for (int64_t b = 0; b < batch; ++b) mx = std::max(mx, hdelta[b]);
@@ -179,10 +213,51 @@ int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, M
   }
   if (iterations) *iterations = it;
   if (converged) *converged = done ? 1 : 0;
-  if (delta_out) QTX_CHECK_CUDA(cudaMemcpyAsync(delta_out, delta, sizeof(double) * batch,
-                                                cudaMemcpyDeviceToDevice, s));
-  QTX_TRY(zinv(n, batch, eps_s, x, info, nullptr, s));
-  if (per_energy) QTX_CHECK_CUDA(cudaStreamSynchronize(s));  // hactive/hdelta stay valid until here
+  return QTX_OK;
+}
+
+}  // namespace
+
+int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
+                     int max_iterations, double tol, int per_energy, int* iterations,
+                     int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s) {
+  SRState st = sr_state(n, batch, ws);
+  if (ws.overflow) {
+    set_error("sancho_rubio: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  QTX_TRY(sr_load(n, batch, 0, st, aii, aij, aji, s));
+  QTX_TRY(sr_iterate(n, batch, st, max_iterations, tol, per_energy, iterations, converged, info, s));
+  if (delta_out)
+    QTX_CHECK_CUDA(cudaMemcpyAsync(delta_out, st.delta, sizeof(double) * batch,
+                                   cudaMemcpyDeviceToDevice, s));
+  QTX_TRY(zinv(n, batch, st.eps_s, x, info, nullptr, s));
+  return QTX_OK;
+}
+
+int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_mat* aii,
+                           const qtx_mat* aij, const qtx_mat* aji, const qtx_mat* x,
+                           int max_iterations, double tol, int per_energy, int* iterations,
+                           int* converged, int* info, Workspace& ws, cudaStream_t s) {
+  int64_t total = 0;
+  for (int k = 0; k < nsys; ++k) total += batches[k];
+  SRState st = sr_state(n, total, ws);
+  if (ws.overflow) {
+    set_error("sancho_rubio_multi: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  int64_t off = 0;
+  for (int k = 0; k < nsys; ++k) {
+    QTX_TRY(sr_load(n, batches[k], off, st, from_abi(aii[k]), from_abi(aij[k]), from_abi(aji[k]), s));
+    off += batches[k];
+  }
+  QTX_TRY(sr_iterate(n, total, st, max_iterations, tol, per_energy, iterations, converged, info, s));
+  off = 0;
+  for (int k = 0; k < nsys; ++k) {
+    QTX_TRY(zinv(n, batches[k], offset(st.eps_s, off), from_abi(x[k]),
+                 info ? info + off : nullptr, nullptr, s));
+    off += batches[k];
+  }
   return QTX_OK;
 }
 

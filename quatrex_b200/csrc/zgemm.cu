@@ -199,13 +199,20 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
           br[j] = v.x;
           bi[j] = (OPB == 1) ? -v.y : v.y;
         }
+        // Two passes over the 2x4 tiles so that the two products feeding one
+        // accumulator are 16 independent MMAs apart (no dependent issue).
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
           for (int j = 0; j < NT; ++j) {
             mma_f64(acc_re[i][j], ar[i][0], ar[i][1], br[j]);
-            mma_f64(acc_re[i][j], nai[i][0], nai[i][1], bi[j]);
             mma_f64(acc_im[i][j], ar[i][0], ar[i][1], bi[j]);
+          }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) {
+            mma_f64(acc_re[i][j], nai[i][0], nai[i][1], bi[j]);
             mma_f64(acc_im[i][j], ai[i][0], ai[i][1], br[j]);
           }
       }

@@ -57,29 +57,39 @@ template <int NB>
 struct Smem {
   static constexpr int PS = NB + 4;  // panel row stride (= 4 mod 8 in 16 B units)
   static constexpr int YS = JW + 2;  // Y row stride (= 2 mod 8)
+  static constexpr int NA = 2 * NB;  // rows a panel's pivoting can touch
   static size_t bytes(int n) {
     size_t s = (size_t)n * PS * sizeof(z64);  // panel
     s += (size_t)NB * YS * sizeof(z64);       // Y tile
+    s += (size_t)NA * JW * sizeof(z64);       // staged old values of the affected rows
     s += (size_t)2 * NB * sizeof(z64);        // scaled pivot row, old row k
     s += (size_t)WARPS * (sizeof(double) + sizeof(int));
-    s += (size_t)2 * n * sizeof(int);  // pivot rows, column sources
+    s += (size_t)3 * NA * sizeof(int);  // affected rows, their sources, source slots
+    s += (size_t)3 * n * sizeof(int);   // pivot rows, column sources, row -> slot map
     return s + 64;
   }
 };
 
 template <int NB>
-__global__ void __launch_bounds__(THREADS) zinv_kernel(int n, int64_t batch, MatRef A, MatRef X,
+__global__ void __launch_bounds__(THREADS, 1) zinv_kernel(int n, int64_t batch, MatRef A, MatRef X,
                                                         int* info, const int* active) {
   using S = Smem<NB>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   z64* P = reinterpret_cast<z64*>(smem_raw);
   z64* Y = P + (size_t)n * S::PS;
-  z64* prow = Y + NB * S::YS;
+  z64* stage = Y + NB * S::YS;
+  z64* prow = stage + S::NA * JW;
   z64* rowk = prow + NB;
   double* red_v = reinterpret_cast<double*>(rowk + NB);
   int* red_i = reinterpret_cast<int*>(red_v + WARPS);
-  int* pivrow = red_i + WARPS;
+  int* aff_row = red_i + WARPS;      // affected row indices
+  int* aff_src = aff_row + S::NA;    // row whose old value each affected row receives
+  int* aff_sslot = aff_src + S::NA;  // slot of that source row in the stage
+  int* pivrow = aff_sslot + S::NA;
   int* colsrc = pivrow + n;
+  int* slot_of = colsrc + n;  // row -> stage slot, -1 if the row is not affected
+
+  for (int r = threadIdx.x; r < n; r += THREADS) slot_of[r] = -1;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -179,74 +189,118 @@ __global__ void __launch_bounds__(THREADS) zinv_kernel(int n, int64_t batch, Mat
         __syncthreads();
       }
 
-      // 3. Apply the panel's row swaps to every column outside the panel.
-      for (int kk = 0; kk < nbp; ++kk) {
-        const int k = k0 + kk;
-        const int p = pivrow[k];
-        if (p != k) {
-          for (int c = tid; c < n; c += THREADS) {
-            if (c >= k0 && c < k0 + nbp) continue;
-            const z64 t = x[(int64_t)k * ldx + c];
-            x[(int64_t)k * ldx + c] = x[(int64_t)p * ldx + c];
-            x[(int64_t)p * ldx + c] = t;
+      // 3. The panel's row interchanges as a permutation of the (at most
+      //    2 NB) rows they touch: affected row aff_row[a] receives the old
+      //    content of row aff_src[a], staged in slot aff_sslot[a].
+      __shared__ int s_na;
+      if (tid == 0) {
+        int na = 0;
+        for (int kk = 0; kk < nbp; ++kk) {
+          const int k = k0 + kk, p = pivrow[k];
+          int ik = slot_of[k], ip = slot_of[p];
+          if (ik < 0) {
+            ik = na++;
+            aff_row[ik] = k;
+            aff_src[ik] = k;
+            slot_of[k] = ik;
           }
+          if (ip < 0) {
+            ip = na++;
+            aff_row[ip] = p;
+            aff_src[ip] = p;
+            slot_of[p] = ip;
+          }
+          const int t = aff_src[ik];
+          aff_src[ik] = aff_src[ip];
+          aff_src[ip] = t;
         }
-        __syncthreads();
+        for (int a = 0; a < na; ++a) aff_sslot[a] = slot_of[aff_src[a]];
+        s_na = na;
       }
+      __syncthreads();
+      const int na = s_na;
 
-      // 4. Trailing update of every other column tile.
+      // 4. Trailing update of every other column tile:
+      //      X[:, J] <- [0 ; X[R, J]] + T[:, K] X[K, J]   (rows permuted).
       for (int j0 = 0; j0 < n; j0 += JW) {
         // Columns of the panel itself are computed but never stored.
         if (j0 >= k0 && j0 + JW <= k0 + nbp) continue;
+        for (int idx = tid; idx < na * JW; idx += THREADS) {
+          const int a = idx / JW, c = idx % JW;
+          const int gc = j0 + c;
+          stage[a * JW + c] = (gc < n && (gc < k0 || gc >= k0 + nbp))
+                                  ? x[(int64_t)aff_row[a] * ldx + gc]
+                                  : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
         for (int idx = tid; idx < NB * JW; idx += THREADS) {
           const int kk = idx / JW, c = idx % JW;
-          Y[kk * S::YS + c] = (kk < nbp && j0 + c < n) ? x[(int64_t)(k0 + kk) * ldx + j0 + c]
-                                                      : make_double2(0.0, 0.0);
+          Y[kk * S::YS + c] =
+              (kk < nbp) ? stage[aff_sslot[slot_of[k0 + kk]] * JW + c] : make_double2(0.0, 0.0);
         }
         __syncthreads();
         const int mtiles = (n + 15) / 16;
-        for (int mt = warp; mt < mtiles; mt += WARPS) {
-          const int r0 = mt * 16;
-          double cre[JW / 8][4], cim[JW / 8][4];
+        for (int base = warp; base < mtiles; base += 2 * WARPS) {
+          double cre[2][JW / 8][4], cim[2][JW / 8][4];
 #pragma unroll
-          for (int j = 0; j < JW / 8; ++j)
+          for (int h = 0; h < 2; ++h) {
+            const int r0 = (base + h * WARPS) * 16;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int r = r0 + g + ((q >> 1) << 3);
-              const int c = j0 + j * 8 + 2 * tq + (q & 1);
-              z64 v = make_double2(0.0, 0.0);
-              if (r < n && c < n && !(r >= k0 && r < k0 + nbp) && (c < k0 || c >= k0 + nbp))
-                v = x[(int64_t)r * ldx + c];
-              cre[j][q] = v.x;
-              cim[j][q] = v.y;
-            }
+            for (int j = 0; j < JW / 8; ++j)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int r = r0 + g + ((q >> 1) << 3);
+                const int cl = j * 8 + 2 * tq + (q & 1);
+                const int c = j0 + cl;
+                z64 v = make_double2(0.0, 0.0);
+                if (r < n && c < n && !(r >= k0 && r < k0 + nbp) && (c < k0 || c >= k0 + nbp)) {
+                  const int sl = slot_of[r];
+                  v = (sl >= 0) ? stage[aff_sslot[sl] * JW + cl] : x[(int64_t)r * ldx + c];
+                }
+                cre[h][j][q] = v.x;
+                cim[h][j][q] = v.y;
+              }
+          }
 #pragma unroll
           for (int k4 = 0; k4 < NB; k4 += 4) {
-            const int ra = r0 + g;
-            const z64 v0 = (ra < n) ? P[ra * S::PS + k4 + tq] : make_double2(0, 0);
-            const z64 v1 = (ra + 8 < n) ? P[(ra + 8) * S::PS + k4 + tq] : make_double2(0, 0);
-            const double nai0 = -v0.y, nai1 = -v1.y;
 #pragma unroll
-            for (int j = 0; j < JW / 8; ++j) {
-              const z64 bv = Y[(k4 + tq) * S::YS + j * 8 + g];
-              mma_f64(cre[j], v0.x, v1.x, bv.x);
-              mma_f64(cre[j], nai0, nai1, bv.y);
-              mma_f64(cim[j], v0.x, v1.x, bv.y);
-              mma_f64(cim[j], v0.y, v1.y, bv.x);
+            for (int h = 0; h < 2; ++h) {
+              const int ra = (base + h * WARPS) * 16 + g;
+              const z64 v0 = (ra < n) ? P[ra * S::PS + k4 + tq] : make_double2(0, 0);
+              const z64 v1 = (ra + 8 < n) ? P[(ra + 8) * S::PS + k4 + tq] : make_double2(0, 0);
+              const double nai0 = -v0.y, nai1 = -v1.y;
+#pragma unroll
+              for (int j = 0; j < JW / 8; ++j) {
+                const z64 bv = Y[(k4 + tq) * S::YS + j * 8 + g];
+                mma_f64(cre[h][j], v0.x, v1.x, bv.x);
+                mma_f64(cim[h][j], v0.x, v1.x, bv.y);
+              }
+#pragma unroll
+              for (int j = 0; j < JW / 8; ++j) {
+                const z64 bv = Y[(k4 + tq) * S::YS + j * 8 + g];
+                mma_f64(cre[h][j], nai0, nai1, bv.y);
+                mma_f64(cim[h][j], v0.y, v1.y, bv.x);
+              }
             }
           }
 #pragma unroll
-          for (int j = 0; j < JW / 8; ++j)
+          for (int h = 0; h < 2; ++h) {
+            const int r0 = (base + h * WARPS) * 16;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int r = r0 + g + ((q >> 1) << 3);
-              const int c = j0 + j * 8 + 2 * tq + (q & 1);
-              if (r < n && c < n && (c < k0 || c >= k0 + nbp))
-                x[(int64_t)r * ldx + c] = make_double2(cre[j][q], cim[j][q]);
-            }
+            for (int j = 0; j < JW / 8; ++j)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int r = r0 + g + ((q >> 1) << 3);
+                const int c = j0 + j * 8 + 2 * tq + (q & 1);
+                if (r < n && c < n && (c < k0 || c >= k0 + nbp))
+                  x[(int64_t)r * ldx + c] = make_double2(cre[h][j][q], cim[h][j][q]);
+              }
+          }
         }
         __syncthreads();
       }
+      if (tid == 0)
+        for (int a = 0; a < na; ++a) slot_of[aff_row[a]] = -1;
 
       // 5. Write the panel back.
       for (int idx = tid; idx < n * nbp; idx += THREADS) {

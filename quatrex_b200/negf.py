@@ -76,11 +76,22 @@ class EnergyPointSolver:
         blocks and every product of the general solve is executed, as in the
         reference. True: it is passed as absent and the products with it are
         skipped (ballistic shortcut).
+    precision : "fp64" or "mixed"
+        "fp64": complex128 throughout (FP64 DMMA products).
+        "mixed": the boundary conditions (Sancho-Rubio, refinement, contact
+        self-energies) stay FP64; the selected solve stores complex64 blocks
+        and runs its products on tcgen05 as split-TF32 products with FP32
+        accumulation, inverting every Schur complement in FP64; the
+        transmission is formed in FP64 from the complex64 corner block.
     """
 
     def __init__(self, h_diag, coupling, eta: float = 1e-4, sr_tol: float = 1e-12,
                  sr_max_iterations: int = 100, per_energy: bool = True,
-                 skip_zero_scattering: bool = False, device: torch.device | None = None):
+                 skip_zero_scattering: bool = False, device: torch.device | None = None,
+                 precision: str = "fp64"):
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.precision = precision
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         h = torch.as_tensor(np.asarray(h_diag), dtype=_C128) if not isinstance(h_diag, torch.Tensor) else h_diag
         t = torch.as_tensor(np.asarray(coupling), dtype=_C128) if not isinstance(coupling, torch.Tensor) else coupling
@@ -89,6 +100,10 @@ class EnergyPointSolver:
         self.upper = (-t).to(self.device, _C128).contiguous()
         self.lower = (-t.conj().transpose(-2, -1)).to(self.device, _C128).contiguous()
         self.zero = torch.zeros((self.b, self.b), dtype=_C128, device=self.device)
+        if precision == "mixed":
+            self.upper64 = self.upper.to(torch.complex64)
+            self.lower64 = self.lower.to(torch.complex64)
+            self.zero64 = torch.zeros((self.b, self.b), dtype=torch.complex64, device=self.device)
         self.eta = float(eta)
         self.sr = SanchoRubio(max_iterations=sr_max_iterations, convergence_tol=sr_tol,
                               per_energy=per_energy)
@@ -103,15 +118,21 @@ class EnergyPointSolver:
             return buf
         N, b, dev = self.N, self.b, self.device
         z = lambda *s: torch.empty(s, dtype=_C128, device=dev)  # noqa: E731
+        ot = torch.complex64 if self.precision == "mixed" else _C128
+        o = lambda *s: torch.empty(s, dtype=ot, device=dev)  # noqa: E731
         buf = dict(
-            a_diag=z(N, B, b, b), xl_d=z(N, B, b, b), xl_u=z(max(N - 1, 1), B, b, b),
-            xl_l=z(max(N - 1, 1), B, b, b), xg_d=z(N, B, b, b), xg_u=z(max(N - 1, 1), B, b, b),
-            xg_l=z(max(N - 1, 1), B, b, b), xr_d=z(N, B, b, b), g0n=z(B, b, b),
+            a_diag=z(N, B, b, b), xl_d=o(N, B, b, b), xl_u=o(max(N - 1, 1), B, b, b),
+            xl_l=o(max(N - 1, 1), B, b, b), xg_d=o(N, B, b, b), xg_u=o(max(N - 1, 1), B, b, b),
+            xg_l=o(max(N - 1, 1), B, b, b), xr_d=o(N, B, b, b), g0n=o(B, b, b),
             gl=z(B, b, b), gr=z(B, b, b), sig=[z(B, b, b) for _ in range(6)],
             current=z(B, N + 1), density=torch.empty((B, N * b), dtype=torch.float64, device=dev),
             T=torch.empty(B, dtype=torch.float64, device=dev), zE=z(B),
             info=torch.zeros(B, dtype=torch.int32, device=dev),
         )
+        if self.precision == "mixed":
+            buf["a_diag64"] = o(N, B, b, b)
+            buf["sig64"] = [o(B, b, b) for _ in range(6)]
+            buf["g0n128"] = z(B, b, b)
         self._bufs = {B: buf}  # keep one batch size resident
         return buf
 
@@ -147,14 +168,13 @@ class EnergyPointSolver:
         #    (A_NN, A_N,N-1, A_N-1,N).
         up, lo = _bcast(self.upper), _bcast(self.lower)
         sig = buf["sig"]
-        iters = []
-        for side, (aii, aij, aji, g, f, s3) in enumerate((
-                (a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
-                (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))):
-            x, it, conv = self._sr(aii, aij, aji, g)
-            iters.append(it)
-            if not conv:
-                warnings.warn("Surface Green's function did not converge.", RuntimeWarning)
+        sides = ((a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
+                 (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))
+        it, conv = self._sr_both(sides, B, stream)
+        if not conv:
+            warnings.warn("Surface Green's function did not converge.", RuntimeWarning)
+        iters = [it, it]
+        for aii, aij, aji, g, f, s3 in sides:
             self._refine(aii, aij, aji, g, B, stream)
             ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
             _native.check(lib.qtx_contact_self_energy(b, B, aij, aji, mat(g), f.data_ptr(), mat(s3[0]),
@@ -163,8 +183,21 @@ class EnergyPointSolver:
 
         # 3. Selected solve.
         keep: list = []
-        A = self._bt([mat(a_diag[i]) for i in range(N)], [up] * (N - 1), [lo] * (N - 1), keep)
-        zs = NULL_MAT if self.skip_zero_scattering else _bcast(self.zero)
+        mixed = self.precision == "mixed"
+        if mixed:
+            for i in range(N):
+                _native.check(lib.qtx_convert(b, b, B, mat(a_diag[i]), _native.QTX_C128,
+                                              mat(buf["a_diag64"][i]), _native.QTX_C64, stream))
+            for k in range(6):
+                _native.check(lib.qtx_convert(b, b, B, mat(sig[k]), _native.QTX_C128, mat(buf["sig64"][k]),
+                                              _native.QTX_C64, stream))
+            ad, sgx = buf["a_diag64"], buf["sig64"]
+            up_s, lo_s, zero = _bcast(self.upper64), _bcast(self.lower64), self.zero64
+        else:
+            ad, sgx = a_diag, sig
+            up_s, lo_s, zero = up, lo, self.zero
+        A = self._bt([mat(ad[i]) for i in range(N)], [up_s] * (N - 1), [lo_s] * (N - 1), keep)
+        zs = NULL_MAT if self.skip_zero_scattering else _bcast(zero)
         S = self._bt([zs] * N, [zs] * (N - 1), [zs] * (N - 1), keep)
         XL = self._bt([mat(buf["xl_d"][i]) for i in range(N)], [mat(buf["xl_u"][i]) for i in range(N - 1)],
                       [mat(buf["xl_l"][i]) for i in range(N - 1)], keep)
@@ -174,36 +207,47 @@ class EnergyPointSolver:
         obc = []
         for k in range(3):
             arr = (QtxMat * N)(*([NULL_MAT] * N))
-            arr[0] = mat(sig[k])
-            arr[N - 1] = mat(sig[3 + k]) if N > 1 else arr[0]
+            arr[0] = mat(sgx[k])
+            arr[N - 1] = mat(sgx[3 + k]) if N > 1 else arr[0]
             obc.append(arr)
         if N == 1:
             raise ValueError("EnergyPointSolver needs at least two blocks")
-        ws_bytes = lib.qtx_selected_solve_workspace(N, A.block_sizes, B, 1)
-        ws = workspace_pool.get(ws_bytes, dev, "rgf")
-        _native.check(lib.qtx_selected_solve(
+        wsq = lib.qtx_selected_solve_mixed_workspace if mixed else lib.qtx_selected_solve_workspace
+        solve = lib.qtx_selected_solve_mixed if mixed else lib.qtx_selected_solve
+        ws = workspace_pool.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
+        _native.check(solve(
             ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
             ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
             buf["density"].data_ptr(), 0, B, buf["info"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
 
-        # 4. Transmission.
+        # 4. Transmission (FP64 from the corner block).
+        g0n = buf["g0n"]
+        if mixed:
+            _native.check(lib.qtx_convert(b, b, B, mat(g0n), _native.QTX_C64, mat(buf["g0n128"]),
+                                          _native.QTX_C128, stream))
+            g0n = buf["g0n128"]
         ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
-        _native.check(lib.qtx_transmission(b, b, B, mat(buf["g0n"]), mat(sig[0]), mat(sig[3]),
+        _native.check(lib.qtx_transmission(b, b, B, mat(g0n), mat(sig[0]), mat(sig[3]),
                                            buf["T"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
         blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
                       xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
         return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], tuple(iters), blocks)
 
-    def _sr(self, aii, aij: QtxMat, aji: QtxMat, out):
+    def _sr_both(self, sides, B: int, stream):
+        """Both contacts' Sancho-Rubio in one decimation loop (2B entries)."""
         lib, dev = self.lib, self.device
-        B = aii.shape[0]
-        ws = workspace_pool.get(lib.qtx_sancho_rubio_workspace(self.b, B), dev, "sr")
+        ws = workspace_pool.get(lib.qtx_sancho_rubio_workspace(self.b, 2 * B), dev, "sr")
         it, conv = ctypes.c_int(0), ctypes.c_int(0)
-        _native.check(lib.qtx_sancho_rubio(
-            self.b, B, mat(aii), aij, aji, mat(out), int(self.sr.max_iterations),
-            float(self.sr.convergence_tol), int(self.sr.per_energy), ctypes.byref(it), ctypes.byref(conv),
-            None, None, ws.data_ptr(), ws.numel(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
-        return out, it.value, bool(conv.value)
+        batches = (ctypes.c_int64 * 2)(B, B)
+        aii = (QtxMat * 2)(mat(sides[0][0]), mat(sides[1][0]))
+        aij = (QtxMat * 2)(sides[0][1], sides[1][1])
+        aji = (QtxMat * 2)(sides[0][2], sides[1][2])
+        x = (QtxMat * 2)(mat(sides[0][3]), mat(sides[1][3]))
+        _native.check(lib.qtx_sancho_rubio_multi(
+            self.b, 2, batches, aii, aij, aji, x, int(self.sr.max_iterations), float(self.sr.convergence_tol),
+            int(self.sr.per_energy), ctypes.byref(it), ctypes.byref(conv), None, ws.data_ptr(), ws.numel(),
+            stream))
+        return it.value, bool(conv.value)
 
     def _refine(self, aii, aij: QtxMat, aji: QtxMat, g, B, stream):
         lib, dev = self.lib, self.device

@@ -99,3 +99,33 @@ def test_memoizer_force_mode_semantics(cuda_device, leads):
     x1 = np.linalg.inv(diag[0] - lower[0] @ x0 @ upper[0])
     x2 = np.linalg.inv(diag[0] - lower[0] @ x1 @ upper[0])
     assert _rel(x, x2) < 1e-10
+
+
+def test_sancho_rubio_multi_matches_single_systems(cuda_device, leads):
+    """Both contacts in one decimation loop equal two separate solves."""
+    import ctypes
+
+    from quatrex_b200 import _native
+    from quatrex_b200._interop import mat
+    from quatrex_b200._native import QtxMat
+
+    _, _, diag, upper, lower = leads
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(cuda_device)  # noqa: E731
+    left = (t(diag[0]), t(upper[0]), t(lower[0]))
+    right = (t(diag[-1]), t(lower[-1]), t(upper[-1]))
+    sr = SanchoRubio(convergence_tol=1e-12, per_energy=True)
+    xl, _, _ = sr.solve_device(*left)
+    xr, _, _ = sr.solve_device(*right)
+    lib = _native.load()
+    B, n = left[0].shape[0], left[0].shape[-1]
+    outs = [torch.empty_like(left[0]), torch.empty_like(right[0])]
+    ws = torch.empty(lib.qtx_sancho_rubio_workspace(n, 2 * B), dtype=torch.uint8, device=cuda_device)
+    it, conv = ctypes.c_int(0), ctypes.c_int(0)
+    _native.check(lib.qtx_sancho_rubio_multi(
+        n, 2, (ctypes.c_int64 * 2)(B, B), (QtxMat * 2)(mat(left[0]), mat(right[0])),
+        (QtxMat * 2)(mat(left[1]), mat(right[1])), (QtxMat * 2)(mat(left[2]), mat(right[2])),
+        (QtxMat * 2)(mat(outs[0]), mat(outs[1])), 100, 1e-12, 1, ctypes.byref(it), ctypes.byref(conv), None,
+        ws.data_ptr(), ws.numel(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    assert conv.value == 1
+    assert _rel(outs[0].cpu().numpy(), xl.cpu().numpy()) < 1e-13
+    assert _rel(outs[1].cpu().numpy(), xr.cpu().numpy()) < 1e-13
