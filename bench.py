@@ -51,7 +51,9 @@ def parse():
     p.add_argument("--cpu-energies", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS FP64 peak measurement")
+    p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS peak measurements")
+    p.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
+                   help="fp64 is the headline value; mixed is reported beside it")
     return p.parse_args()
 
 
@@ -114,6 +116,29 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
                 "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_tf32_peak(torch, device) -> float:
+    """cuBLAS FP32 GEMM with TF32 tensor cores, 8192^3, best of 5 (TFLOP/s)."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    n = 8192
+    a = torch.randn((n, n), dtype=torch.float32, device=device)
+    b = torch.randn((n, n), dtype=torch.float32, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    torch.backends.cuda.matmul.allow_tf32 = old
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
 def measured_fp64_peak(torch, device) -> dict:
@@ -287,48 +312,66 @@ def run_ours(args, world, rank, local):
     B = min(args.batch, mine.size)
     batches = [mine[i:i + B] for i in range(0, mine.size - B + 1, B)] or [mine]
     fl_all, fr_all = dev.fermi_left(), dev.fermi_right()
-    solver = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True,
-                               device=device)
     lib = _native.load()
-
-    def step(k):
-        idx = batches[k % len(batches)]
-        return solver.solve(dev.energies[idx], fl_all[idx], fr_all[idx])
-
     peak = {"peak": None} if args.no_peak else measured_fp64_peak(torch, device)
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-
+    tf32_peak = None if (args.no_peak or args.precision == "fp64") else measured_tf32_peak(torch, device)
     props = torch.cuda.get_device_properties(device)
     gpu_id = str(getattr(props, "uuid", local))
     if gpu_id and not gpu_id.startswith("GPU-") and len(gpu_id) > 8:
         gpu_id = "GPU-" + gpu_id
-    clocks = ClockSampler(gpu_id)
-    lib.qtx_profile_reset()
-    lib.qtx_profile_enable(1)
-    sr_iters = []
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record()
-    for k in range(args.steps):
-        r = step(args.warmup + k)
-        sr_iters.append(r.sr_iterations)
-    t_end.record()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    lib.qtx_profile_enable(0)
-    ms = t_start.elapsed_time(t_end)
-    gemm_ms, gemm_flops, gemm_n = _native.profile_read(0)
-    inv_ms, inv_flops, inv_n = _native.profile_read(1)
-    all_ms, _, all_n = _native.profile_read(-1)
-    lib.qtx_profile_reset()
+
+    def timed(precision):
+        solver = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True,
+                                   device=device, precision=precision)
+
+        def step(k):
+            idx = batches[k % len(batches)]
+            return solver.solve(dev.energies[idx], fl_all[idx], fr_all[idx])
+
+        for k in range(args.warmup):
+            step(k)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(gpu_id)
+        lib.qtx_profile_reset()
+        lib.qtx_profile_enable(1)
+        sr_iters = []
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for k in range(args.steps):
+            r = step(args.warmup + k)
+            sr_iters.append(r.sr_iterations)
+        t_end.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop()
+        lib.qtx_profile_enable(0)
+        ms = t_start.elapsed_time(t_end)
+        prof = {name: _native.profile_read(kind) for name, kind in _native.KERNEL_CLASSES.items()}
+        prof["all"] = _native.profile_read(-1)
+        lib.qtx_profile_reset()
+        # a fixed probe batch for cross-precision error reporting
+        probe = batches[0]
+        rp = solver.solve(dev.energies[probe], fl_all[probe], fr_all[probe])
+        torch.cuda.synchronize()
+        probe_out = (rp.transmission.cpu().numpy().copy(), rp.density.cpu().numpy().copy())
+        del solver
+        torch.cuda.empty_cache()
+        return ms, prof, clk, sr_iters, probe_out
+
+    res = {}
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+        res[prec] = timed(prec)
+    main_prec = "fp64" if "fp64" in res else "mixed"
+    ms, prof, clk, sr_iters, _ = res[main_prec]
+    gemm_ms, gemm_flops, gemm_n = prof["zgemm"] if main_prec == "fp64" else prof["cgemm"]
+    inv_ms, inv_flops, inv_n = prof["zinv"]
+    all_ms, _, all_n = prof["all"]
 
     t = torch.tensor([ms], dtype=torch.float64, device=device)
     if world > 1:
@@ -339,6 +382,35 @@ def run_ours(args, world, rank, local):
     if world > 1:
         dist.all_reduce(total)
     value = float(total.item()) / (ms_max * 1e-3)
+
+    mixed_line = None
+    if "mixed" in res and main_prec == "fp64":
+        mms, mprof, mclk, _, mprobe = res["mixed"]
+        tm = torch.tensor([mms], dtype=torch.float64, device=device)
+        if world > 1:
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        cg_ms, cg_flops, cg_n = mprof["cgemm"]
+        ach = (cg_flops / cg_n) / ((cg_ms / cg_n) * 1e-3) / 1e12 if cg_n else None
+        fprobe = res["fp64"][4]
+        terr = np.abs(mprobe[0] - fprobe[0]) / np.abs(fprobe[0])
+        mixed_line = {
+            "value": float(total.item()) / (float(tm.item()) * 1e-3), "unit": UNIT,
+            "ms_per_step": float(tm.item()) / args.steps,
+            "speedup_vs_fp64": ms_max / float(tm.item()),
+            "dtype": "c64 storage; tcgen05 split-TF32 products, FP32 accumulation; FP64 inverses and OBC",
+            "roofline": {"bound": "tensor", "kernel": "cgemm_tc (tcgen05 kind::tf32, 12 MMAs per complex K step)",
+                         "achieved": ach, "peak": tf32_peak, "unit": "TFLOP/s (complex as-written 8mnk)",
+                         "frac": (ach / tf32_peak) if (ach and tf32_peak) else None,
+                         "peak_source": "measured cuBLAS FP32 GEMM with TF32 tensor cores 8192^3 on this GPU",
+                         "launches": cg_n, "avg_launch_ms": cg_ms / cg_n if cg_n else None,
+                         "share_of_step_time": cg_ms / mms if mms else None,
+                         "zinv_ms_share": mprof["zinv"][0] / mms if mms else None},
+            "error_vs_fp64": {"transmission_max_rel": float(terr.max()),
+                              "transmission_median_rel": float(np.median(terr)),
+                              "density_rel": float(np.linalg.norm(mprobe[1] - fprobe[1]) / np.linalg.norm(fprobe[1])),
+                              "probe": f"{batches[0].size} energies of the grid"},
+            "gpu_launches": mprof["all"][2], "clocks": mclk,
+        }
 
     e2e = None
     cpu = None
@@ -381,6 +453,7 @@ def run_ours(args, world, rank, local):
         "e2e": e2e,
         "gpu_launches": all_n,
         "clocks": clk,
+        "mixed": mixed_line,
     }
     print(json.dumps(line), flush=True)
 

@@ -207,6 +207,19 @@ int qtx_sancho_rubio_multi(int n, int num_systems, const int64_t* batches, const
                            int* converged, int* info, void* workspace, size_t workspace_bytes,
                            qtx_stream stream);
 
+/* qtx_sancho_rubio_multi without host synchronisation: exactly
+ * max_iterations decimation steps are enqueued; convergence is tracked on
+ * the device (per-energy or batch-wide, as per_energy selects) and retired
+ * entries are skipped by every later kernel, so converged steps cost only
+ * their launches. The whole sequence can be captured in a CUDA graph.
+ * d_iterations / d_converged: device ints receiving the number of steps that
+ * still had active entries and whether all entries met the tolerance. */
+int qtx_sancho_rubio_multi_async(int n, int num_systems, const int64_t* batches,
+                                 const qtx_mat* a_ii, const qtx_mat* a_ij, const qtx_mat* a_ji,
+                                 const qtx_mat* x, int max_iterations, double tol, int per_energy,
+                                 int* d_iterations, int* d_converged, int* info, void* workspace,
+                                 size_t workspace_bytes, qtx_stream stream);
+
 /* Workspace bytes sufficient for qtx_contact_self_energy, qtx_obc_refine
  * and qtx_transmission (square n x n blocks) on `batch` entries. */
 size_t qtx_obc_workspace(int n, int64_t batch);
@@ -251,6 +264,11 @@ int qtx_coo_densify(int64_t batch, const void* data, int64_t data_stride, int64_
  * data[b * data_stride + k] = in[b, rows[k], cols[k]]. */
 int qtx_coo_sparsify(int64_t batch, qtx_mat in, int64_t nnz, const int32_t* rows,
                      const int32_t* cols, void* data, int64_t data_stride, qtx_stream stream);
+
+/* Complex energies z[b] = E[b] + i eta (device double[batch] in, device
+ * complex128[batch] out), the scalar part of the system-matrix assembly. */
+int qtx_assemble_energies(int64_t batch, const double* energies, double eta, void* z,
+                          qtx_stream stream);
 
 /* Diagonal blocks of the system matrix, out[b] = z[b] I - h[b]
  * (the assembly of quatrex/electron/solver.py:668-709 with zero potential

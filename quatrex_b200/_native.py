@@ -76,6 +76,9 @@ SIGNATURES = {
     "qtx_sancho_rubio_multi": (c_int, [c_int, c_int, POINTER(c_int64), POINTER(QtxMat), POINTER(QtxMat),
                                        POINTER(QtxMat), POINTER(QtxMat), c_int, c_double, c_int, POINTER(c_int),
                                        POINTER(c_int), c_void_p, c_void_p, c_size_t, c_void_p]),
+    "qtx_sancho_rubio_multi_async": (c_int, [c_int, c_int, POINTER(c_int64), POINTER(QtxMat), POINTER(QtxMat),
+                                             POINTER(QtxMat), POINTER(QtxMat), c_int, c_double, c_int, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "qtx_obc_workspace": (c_size_t, [c_int, c_int64]),
     "qtx_contact_self_energy": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, c_void_p, QtxMat, QtxMat,
                                         QtxMat, c_void_p, c_size_t, c_void_p]),
@@ -90,6 +93,7 @@ SIGNATURES = {
     "qtx_profile_enable": (c_int, [c_int]),
     "qtx_profile_reset": (c_int, []),
     "qtx_profile_read": (c_int, [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]),
+    "qtx_assemble_energies": (c_int, [c_int64, c_void_p, c_double, c_void_p, c_void_p]),
     "qtx_assemble_diag": (c_int, [c_int, c_int64, QtxMat, c_void_p, QtxMat, c_void_p]),
 }
 

@@ -33,6 +33,10 @@ int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_ma
                            const qtx_mat* aij, const qtx_mat* aji, const qtx_mat* x,
                            int max_iterations, double tol, int per_energy, int* iterations,
                            int* converged, int* info, Workspace& ws, cudaStream_t s);
+int sancho_rubio_multi_async_run(int n, int nsys, const int64_t* batches, const qtx_mat* aii,
+                                 const qtx_mat* aij, const qtx_mat* aji, const qtx_mat* x,
+                                 int max_iterations, double tol, int per_energy, int* d_iters,
+                                 int* d_converged, int* info, Workspace& ws, cudaStream_t s);
 size_t obc_refine_ws(int n, int64_t batch);
 int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x, MatRef xref,
                    double* rel, double* abs_res, int* info, Workspace& ws, cudaStream_t s);
@@ -414,6 +418,36 @@ int qtx_sancho_rubio_multi(int n, int num_systems, const int64_t* batches, const
     Workspace ws = bind(workspace, workspace_bytes);
     return sancho_rubio_multi_run(n, num_systems, batches, a_ii, a_ij, a_ji, x, max_iterations, tol,
                                   per_energy, iterations, converged, info, ws, s);
+  });
+}
+
+int qtx_sancho_rubio_multi_async(int n, int num_systems, const int64_t* batches,
+                                 const qtx_mat* a_ii, const qtx_mat* a_ij, const qtx_mat* a_ji,
+                                 const qtx_mat* x, int max_iterations, double tol, int per_energy,
+                                 int* d_iterations, int* d_converged, int* info, void* workspace,
+                                 size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (n <= 0 || n > 1024 || num_systems <= 0 || batches == nullptr || a_ii == nullptr ||
+        a_ij == nullptr || a_ji == nullptr || x == nullptr || max_iterations < 0 ||
+        d_iterations == nullptr || d_converged == nullptr) {
+      set_error("qtx_sancho_rubio_multi_async: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    int64_t total = 0;
+    for (int k = 0; k < num_systems; ++k) {
+      if (batches[k] <= 0 || a_ii[k].ptr == nullptr || x[k].ptr == nullptr) {
+        set_error("qtx_sancho_rubio_multi_async: empty system or null matrix");
+        return (int)QTX_ERR_ARG;
+      }
+      total += batches[k];
+    }
+    QTX_TRY(need_ws(workspace, workspace_bytes, sancho_rubio_ws(n, total),
+                    "qtx_sancho_rubio_multi_async"));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * total, s));
+    Workspace ws = bind(workspace, workspace_bytes);
+    return sancho_rubio_multi_async_run(n, num_systems, batches, a_ii, a_ij, a_ji, x, max_iterations,
+                                        tol, per_energy, d_iterations, d_converged, info, ws, s);
   });
 }
 

@@ -133,3 +133,28 @@ extern "C" int qtx_assemble_diag(int n, int64_t batch, qtx_mat h, const void* z,
   QTX_CHECK_LAUNCH();
   return QTX_OK;
 }
+
+// z[b] = E[b] + i eta: the complex energies of one batch.
+namespace qtx {
+namespace {
+__global__ void energies_kernel(int64_t batch, const double* E, double eta, z64* z) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < batch;
+       b += (int64_t)gridDim.x * blockDim.x)
+    z[b] = make_double2(E[b], eta);
+}
+}  // namespace
+}  // namespace qtx
+
+extern "C" int qtx_assemble_energies(int64_t batch, const double* energies, double eta, void* z,
+                                     qtx_stream stream) {
+  if (batch <= 0) return QTX_OK;
+  if (energies == nullptr || z == nullptr) {
+    set_error("qtx_assemble_energies: null argument");
+    return QTX_ERR_ARG;
+  }
+  ProfScope prof(QTX_KERNEL_FORMAT, 24.0 * (double)batch, (cudaStream_t)stream);
+  energies_kernel<<<blocks_for(batch), 256, 0, (cudaStream_t)stream>>>(batch, energies, eta,
+                                                                        static_cast<z64*>(z));
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}

@@ -216,7 +216,127 @@ int sr_iterate(int n, int64_t batch, const SRState& st, int max_iterations, doub
   return QTX_OK;
 }
 
+// Device-side convergence bookkeeping of one decimation step (one CTA):
+// per-energy mode retires entries whose delta is below tol; batch-wide mode
+// retires all once the largest active delta is below tol. Counts the step
+// if any entry was still active and records whether all have converged.
+__global__ void __launch_bounds__(256) sr_update_kernel(int64_t batch, const double* delta, int* active,
+                                                         double tol, int per_energy, int* iters,
+                                                         int* converged) {
+  __shared__ double s_max[8];
+  __shared__ int s_any[8], s_left[8];
+  double mx = 0.0;
+  int any = 0;
+  for (int64_t b = threadIdx.x; b < batch; b += blockDim.x)
+    if (active[b]) {
+      any = 1;
+      mx = fmax(mx, delta[b]);
+    }
+  for (int off = 16; off > 0; off >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    any |= __shfl_xor_sync(0xffffffffu, any, off);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    s_max[w] = mx;
+    s_any[w] = any;
+  }
+  __syncthreads();
+  mx = 0.0;
+  any = 0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+    mx = fmax(mx, s_max[k]);
+    any |= s_any[k];
+  }
+  int left = 0;
+  for (int64_t b = threadIdx.x; b < batch; b += blockDim.x) {
+    if (!active[b]) continue;
+    const bool done = per_energy ? (delta[b] < tol) : (mx < tol);
+    if (done)
+      active[b] = 0;
+    else
+      ++left;
+  }
+  for (int off = 16; off > 0; off >>= 1) left += __shfl_xor_sync(0xffffffffu, left, off);
+  __syncthreads();
+  if (l == 0) s_left[w] = left;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tot += s_left[k];
+    if (any) *iters += 1;
+    *converged = (tot == 0) ? 1 : 0;
+  }
+}
+
+// Host-sync-free decimation: max_iterations steps are enqueued; once every
+// entry has retired the remaining steps' kernels find no active entry and
+// return at once. d_iters / d_converged are device ints.
+int sr_iterate_async(int n, int64_t batch, const SRState& st, int max_iterations, double tol,
+                     int per_energy, int* d_iters, int* d_converged, int* info, cudaStream_t s) {
+  QTX_TRY(fill_int(st.active, batch, 1, s));
+  QTX_TRY(fill_int(d_iters, 1, 0, s));
+  QTX_TRY(fill_int(d_converged, 1, 0, s));
+  int cur = 0;
+  const int* mask = st.active;
+  for (int it = 0; it < max_iterations; ++it) {
+    const int nx = cur ^ 1;
+    QTX_TRY(zinv(n, batch, st.eps, st.inv_e, info, mask, s));
+    QTX_TRY(G(n, n, n, batch, st.alpha[cur], st.inv_e, st.aI).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.beta[cur], st.inv_e, st.bI).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.aI, st.beta[cur], st.t1)
+                .second(st.eps_s, MONE)
+                .plus3(st.eps_s, ONE)
+                .mask(mask)
+                .run(s));
+    QTX_TRY(G(n, n, n, batch, st.bI, st.alpha[cur], st.eps, MONE)
+                .plus(st.eps, ONE)
+                .plus(st.t1, MONE)
+                .mask(mask)
+                .run(s));
+    QTX_TRY(G(n, n, n, batch, st.aI, st.alpha[cur], st.alpha[nx]).mask(mask).run(s));
+    QTX_TRY(G(n, n, n, batch, st.bI, st.beta[cur], st.beta[nx]).mask(mask).run(s));
+    QTX_TRY(sr_delta(n, batch, st.alpha[nx], st.beta[nx], st.delta, mask, s));
+    {
+      ProfScope prof(QTX_KERNEL_REDUCE, 12.0 * (double)batch, s);
+      sr_update_kernel<<<1, 256, 0, s>>>(batch, st.delta, st.active, tol, per_energy, d_iters,
+                                         d_converged);
+      QTX_CHECK_LAUNCH();
+    }
+    cur = nx;
+  }
+  // Entries retired in different steps left their newest alpha/beta in
+  // different buffers; eps_s (updated in place) is all that is read next.
+  return QTX_OK;
+}
+
 }  // namespace
+
+int sancho_rubio_multi_async_run(int n, int nsys, const int64_t* batches, const qtx_mat* aii,
+                                 const qtx_mat* aij, const qtx_mat* aji, const qtx_mat* x,
+                                 int max_iterations, double tol, int per_energy, int* d_iters,
+                                 int* d_converged, int* info, Workspace& ws, cudaStream_t s) {
+  int64_t total = 0;
+  for (int k = 0; k < nsys; ++k) total += batches[k];
+  SRState st = sr_state(n, total, ws);
+  if (ws.overflow) {
+    set_error("sancho_rubio_multi_async: workspace too small");
+    return QTX_ERR_WORKSPACE;
+  }
+  int64_t off = 0;
+  for (int k = 0; k < nsys; ++k) {
+    QTX_TRY(sr_load(n, batches[k], off, st, from_abi(aii[k]), from_abi(aij[k]), from_abi(aji[k]), s));
+    off += batches[k];
+  }
+  QTX_TRY(sr_iterate_async(n, total, st, max_iterations, tol, per_energy, d_iters, d_converged, info, s));
+  off = 0;
+  for (int k = 0; k < nsys; ++k) {
+    QTX_TRY(zinv(n, batches[k], offset(st.eps_s, off), from_abi(x[k]), info ? info + off : nullptr,
+                 nullptr, s));
+    off += batches[k];
+  }
+  return QTX_OK;
+}
 
 int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x,
                      int max_iterations, double tol, int per_energy, int* iterations,

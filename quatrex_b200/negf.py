@@ -76,6 +76,10 @@ class EnergyPointSolver:
         blocks and every product of the general solve is executed, as in the
         reference. True: it is passed as absent and the products with it are
         skipped (ballistic shortcut).
+    device_loop : bool
+        Run Sancho-Rubio with device-side convergence (no host
+        synchronisation; required for CUDA-graph capture). The host-driven
+        loop (default) stops at exactly the reference's iteration.
     precision : "fp64" or "mixed"
         "fp64": complex128 throughout (FP64 DMMA products).
         "mixed": the boundary conditions (Sancho-Rubio, refinement, contact
@@ -88,7 +92,7 @@ class EnergyPointSolver:
     def __init__(self, h_diag, coupling, eta: float = 1e-4, sr_tol: float = 1e-12,
                  sr_max_iterations: int = 100, per_energy: bool = True,
                  skip_zero_scattering: bool = False, device: torch.device | None = None,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", device_loop: bool = False):
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -108,7 +112,11 @@ class EnergyPointSolver:
         self.sr = SanchoRubio(max_iterations=sr_max_iterations, convergence_tol=sr_tol,
                               per_energy=per_energy)
         self.skip_zero_scattering = skip_zero_scattering
+        self.device_loop = device_loop
         self._bufs: dict = {}
+        self._graphs: dict = {}
+        self._host_sr = (0, True)
+        self._last_device_loop = device_loop
         self.lib = _native.load()
 
     # ------------------------------------------------------------------
@@ -128,11 +136,18 @@ class EnergyPointSolver:
             current=z(B, N + 1), density=torch.empty((B, N * b), dtype=torch.float64, device=dev),
             T=torch.empty(B, dtype=torch.float64, device=dev), zE=z(B),
             info=torch.zeros(B, dtype=torch.int32, device=dev),
+            E=torch.empty(B, dtype=torch.float64, device=dev), fl=torch.empty(B, dtype=torch.float64, device=dev),
+            fr=torch.empty(B, dtype=torch.float64, device=dev),
+            res_rel=[torch.empty(B, dtype=torch.float64, device=dev) for _ in range(2)],
+            res_abs=[torch.empty(B, dtype=torch.float64, device=dev) for _ in range(2)],
+            sr_it=torch.zeros(1, dtype=torch.int32, device=dev), sr_conv=torch.zeros(1, dtype=torch.int32, device=dev),
         )
         if self.precision == "mixed":
             buf["a_diag64"] = o(N, B, b, b)
             buf["sig64"] = [o(B, b, b) for _ in range(6)]
             buf["g0n128"] = z(B, b, b)
+        if self._bufs:
+            self._graphs.clear()  # graphs refer to the buffers being replaced
         self._bufs = {B: buf}  # keep one batch size resident
         return buf
 
@@ -148,15 +163,80 @@ class EnergyPointSolver:
     # ------------------------------------------------------------------
     def solve(self, energies, f_left, f_right) -> PointResult:
         """Solves one batch of energies; all results stay on the device."""
-        lib, dev = self.lib, self.device
-        N, b = self.N, self.b
-        E = torch.as_tensor(energies, dtype=torch.float64, device=dev).reshape(-1)
+        B = self.set_inputs(energies, f_left, f_right)
+        res = self._run(B, device_loop=self.device_loop)
+        if not self.device_loop:
+            it, conv = self._host_sr
+            if not conv:
+                warnings.warn("Surface Green's function did not converge.", RuntimeWarning)
+        return res
+
+    def set_inputs(self, energies, f_left, f_right) -> int:
+        """Copies one batch's energies and occupations into the solver's
+        device input buffers (the only per-batch host-to-device traffic)."""
+        dev = self.device
+        E = torch.as_tensor(np.asarray(energies, dtype=np.float64)).reshape(-1)
         B = int(E.numel())
         buf = self._buffers(B)
+        buf["E"].copy_(E, non_blocking=False)
+        buf["fl"].copy_(torch.as_tensor(np.asarray(f_left, dtype=np.float64)).reshape(-1))
+        buf["fr"].copy_(torch.as_tensor(np.asarray(f_right, dtype=np.float64)).reshape(-1))
+        return B
+
+    def capture(self, B: int) -> "torch.cuda.CUDAGraph":
+        """Captures the whole energy-point pipeline for batch size B in one
+        CUDA graph (Sancho-Rubio runs its device-side convergence loop). The
+        inputs are read from the solver's device buffers, so a replay after
+        set_inputs() solves a new batch. The first capture runs the pipeline
+        once eagerly to allocate every buffer outside the capture."""
+        g = self._graphs.get(B)
+        if g is not None:
+            return g
+        self._buffers(B)
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self._run(B, device_loop=True)
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self._run(B, device_loop=True)
+        self._graphs[B] = g
+        return g
+
+    def solve_graph(self, energies, f_left, f_right) -> PointResult:
+        """solve() through the captured CUDA graph of this batch size."""
+        B = self.set_inputs(energies, f_left, f_right)
+        g = self.capture(B)
+        g.replay()
+        return self._result(B)
+
+    def sr_status(self, B: int) -> tuple[int, bool]:
+        """(decimation steps, converged) of the last device-loop run."""
+        buf = self._buffers(B)
+        return int(buf["sr_it"].item()), bool(buf["sr_conv"].item())
+
+    def _result(self, B: int) -> PointResult:
+        buf = self._bufs[B]
+        sig = buf["sig"]
+        blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
+                      xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
+        its = (self._host_sr[0],) * 2 if not self._last_device_loop else ("device", "device")
+        return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], its, blocks)
+
+    def _run(self, B: int, device_loop: bool) -> PointResult:
+        """The kernel sequence of one batch; no host transfers, and no host
+        synchronisation when device_loop is set (graph-capturable)."""
+        lib, dev = self.lib, self.device
+        N, b = self.N, self.b
+        buf = self._bufs[B]
         stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
-        buf["zE"].copy_(E.to(_C128) + 1j * self.eta)
-        fl = torch.as_tensor(f_left, dtype=torch.float64, device=dev).reshape(-1).contiguous()
-        fr = torch.as_tensor(f_right, dtype=torch.float64, device=dev).reshape(-1).contiguous()
+        keep: list = []
+        self._last_device_loop = device_loop
+        fl, fr = buf["fl"], buf["fr"]
+        _native.check(lib.qtx_assemble_energies(B, buf["E"].data_ptr(), float(self.eta), buf["zE"].data_ptr(),
+                                                stream))
 
         # 1. A(E) diagonal blocks.
         a_diag = buf["a_diag"]
@@ -170,19 +250,19 @@ class EnergyPointSolver:
         sig = buf["sig"]
         sides = ((a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
                  (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))
-        it, conv = self._sr_both(sides, B, stream)
-        if not conv:
-            warnings.warn("Surface Green's function did not converge.", RuntimeWarning)
-        iters = [it, it]
-        for aii, aij, aji, g, f, s3 in sides:
-            self._refine(aii, aij, aji, g, B, stream)
+        self._sr_both(sides, B, stream, device_loop, buf)
+        for k, (aii, aij, aji, g, f, s3) in enumerate(sides):
             ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
+            _native.check(lib.qtx_obc_refine(b, B, mat(aii), aij, aji, mat(g), mat(g),
+                                             buf["res_rel"][k].data_ptr(), buf["res_abs"][k].data_ptr(), None,
+                                             ws.data_ptr(), ws.numel(), stream))
             _native.check(lib.qtx_contact_self_energy(b, B, aij, aji, mat(g), f.data_ptr(), mat(s3[0]),
                                                       mat(s3[1]), mat(s3[2]), ws.data_ptr(), ws.numel(),
                                                       stream))
+        self.last_residuals = (torch.maximum(buf["res_rel"][0], buf["res_rel"][1]) if not device_loop
+                               else buf["res_rel"][0], buf["res_abs"][0])
 
         # 3. Selected solve.
-        keep: list = []
         mixed = self.precision == "mixed"
         if mixed:
             for i in range(N):
@@ -208,10 +288,8 @@ class EnergyPointSolver:
         for k in range(3):
             arr = (QtxMat * N)(*([NULL_MAT] * N))
             arr[0] = mat(sgx[k])
-            arr[N - 1] = mat(sgx[3 + k]) if N > 1 else arr[0]
+            arr[N - 1] = mat(sgx[3 + k])
             obc.append(arr)
-        if N == 1:
-            raise ValueError("EnergyPointSolver needs at least two blocks")
         wsq = lib.qtx_selected_solve_mixed_workspace if mixed else lib.qtx_selected_solve_workspace
         solve = lib.qtx_selected_solve_mixed if mixed else lib.qtx_selected_solve
         ws = workspace_pool.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
@@ -229,34 +307,29 @@ class EnergyPointSolver:
         ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
         _native.check(lib.qtx_transmission(b, b, B, mat(g0n), mat(sig[0]), mat(sig[3]),
                                            buf["T"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
-        blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
-                      xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
-        return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], tuple(iters), blocks)
+        return self._result(B)
 
-    def _sr_both(self, sides, B: int, stream):
+    def _sr_both(self, sides, B: int, stream, device_loop: bool, buf):
         """Both contacts' Sancho-Rubio in one decimation loop (2B entries)."""
         lib, dev = self.lib, self.device
         ws = workspace_pool.get(lib.qtx_sancho_rubio_workspace(self.b, 2 * B), dev, "sr")
-        it, conv = ctypes.c_int(0), ctypes.c_int(0)
         batches = (ctypes.c_int64 * 2)(B, B)
         aii = (QtxMat * 2)(mat(sides[0][0]), mat(sides[1][0]))
         aij = (QtxMat * 2)(sides[0][1], sides[1][1])
         aji = (QtxMat * 2)(sides[0][2], sides[1][2])
         x = (QtxMat * 2)(mat(sides[0][3]), mat(sides[1][3]))
+        if device_loop:
+            _native.check(lib.qtx_sancho_rubio_multi_async(
+                self.b, 2, batches, aii, aij, aji, x, int(self.sr.max_iterations), float(self.sr.convergence_tol),
+                int(self.sr.per_energy), buf["sr_it"].data_ptr(), buf["sr_conv"].data_ptr(), None, ws.data_ptr(),
+                ws.numel(), stream))
+            return
+        it, conv = ctypes.c_int(0), ctypes.c_int(0)
         _native.check(lib.qtx_sancho_rubio_multi(
             self.b, 2, batches, aii, aij, aji, x, int(self.sr.max_iterations), float(self.sr.convergence_tol),
             int(self.sr.per_energy), ctypes.byref(it), ctypes.byref(conv), None, ws.data_ptr(), ws.numel(),
             stream))
-        return it.value, bool(conv.value)
-
-    def _refine(self, aii, aij: QtxMat, aji: QtxMat, g, B, stream):
-        lib, dev = self.lib, self.device
-        ws = workspace_pool.get(lib.qtx_obc_workspace(self.b, B), dev, "obc")
-        rel = torch.empty(B, dtype=torch.float64, device=dev)
-        ab = torch.empty(B, dtype=torch.float64, device=dev)
-        _native.check(lib.qtx_obc_refine(self.b, B, mat(aii), aij, aji, mat(g), mat(g), rel.data_ptr(),
-                                         ab.data_ptr(), None, ws.data_ptr(), ws.numel(), stream))
-        self.last_residuals = (rel, ab)
+        self._host_sr = (it.value, bool(conv.value))
 
 
 def flops_per_energy(N: int, b: int, sr_iterations: tuple = (0, 0)) -> dict:

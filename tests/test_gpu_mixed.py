@@ -1,7 +1,7 @@
 """The mixed-precision path: complex64 GEMM on tcgen05 with split-TF32
-products and FP32 accumulation. Tolerance: 5e-6 relative to the complex128
-product (FP32-level; the split recovers ~21 of FP32's 24 mantissa bits and
-accumulation is FP32)."""
+products and FP32 accumulation. Tolerance: max(5e-6, 5e-7 sqrt(K)) relative
+to the complex128 product (FP32-level: the split recovers ~21 of FP32's 24
+mantissa bits and the FP32 accumulation error grows like sqrt(K))."""
 
 import ctypes
 
@@ -49,7 +49,7 @@ def test_cgemm_tc_matches_complex128(cuda_device, m, n, k, op_a, op_b):
     assert int(err.item()) == 0
     got = C.cpu().numpy().astype(np.complex128)
     rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
-    assert rel < TOL, rel
+    assert rel < max(TOL, 5e-7 * np.sqrt(k)), rel
 
 
 def _rel(a, b):
