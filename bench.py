@@ -427,23 +427,33 @@ def run_ours(args, world, rank, local):
         return
 
     achieved = (gemm_flops / gemm_n) / ((gemm_ms / gemm_n) * 1e-3) / 1e12 if gemm_n else None
-    roofline = {"bound": "tensor", "kernel": "zgemm (batched complex128 DMMA)", "achieved": achieved,
-                "peak": peak["peak"], "unit": "TFLOP/s",
-                "frac": (achieved / peak["peak"]) if achieved and peak["peak"] else None,
-                "peak_source": "measured cuBLAS FP64 (max of DGEMM 8192^3, ZGEMM 4096^3) on this GPU; "
-                               "no FP64 entry in MEASURED_PEAKS.json",
-                "peak_detail": peak, "traffic": _ncu_traffic(), "launches": gemm_n,
-                "avg_launch_ms": gemm_ms / gemm_n if gemm_n else None,
-                "share_of_step_time": gemm_ms / ms if ms else None,
-                "zinv_ms_share": inv_ms / ms if ms else None}
+    if main_prec == "fp64":
+        roofline = {"bound": "tensor", "kernel": "zgemm (batched complex128 DMMA)", "achieved": achieved,
+                    "peak": peak["peak"], "unit": "TFLOP/s",
+                    "frac": (achieved / peak["peak"]) if achieved and peak["peak"] else None,
+                    "peak_source": "measured cuBLAS FP64 (max of DGEMM 8192^3, ZGEMM 4096^3) on this GPU; "
+                                   "no FP64 entry in MEASURED_PEAKS.json",
+                    "peak_detail": peak, "traffic": _ncu_traffic(), "launches": gemm_n}
+    else:
+        roofline = {"bound": "tensor", "kernel": "cgemm_tc (tcgen05 kind::tf32, 12 MMAs per complex K step)",
+                    "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s (complex as-written 8mnk)",
+                    "frac": (achieved / tf32_peak) if achieved and tf32_peak else None,
+                    "peak_source": "measured cuBLAS FP32 GEMM with TF32 tensor cores 8192^3 on this GPU",
+                    "traffic": None, "launches": gemm_n}
+    roofline.update({"avg_launch_ms": gemm_ms / gemm_n if gemm_n else None,
+                     "share_of_step_time": gemm_ms / ms if ms else None,
+                     "zinv_ms_share": inv_ms / ms if ms else None})
     from quatrex_b200.negf import flops_per_energy
 
     its = np.mean(np.array(sr_iters), axis=0) if sr_iters else (0, 0)
     fl = flops_per_energy(32, 256, tuple(float(x) for x in its))
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if main_prec == "fp64" else METRIC.replace("(FP64)", "(mixed)"),
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (complex128)" if main_prec == "fp64" else "c64 storage, split-TF32 products",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "batch": B, "energies": args.energies,
                    "parallelism": f"energy sharding x{world}", "l2": "inputs exceed L2 (resident batch state "
                    f"~{B * 0.45:.0f} GB)", "sr_iterations_mean": [float(x) for x in its]},

@@ -10,11 +10,11 @@
 // negate bit: 12 tcgen05.mma.kind::tf32 per K step of 8.
 //
 // CTA tile 128 x 64 (one UMMA M=128, N=64), K block 32 FP32 (128-byte rows,
-// SWIZZLE_128B K-major). The raw complex64 tiles of the next-but-one K block
-// stream into a double-buffered staging area with cp.async while the current
-// block is split in shared memory (raw -> hi/lo planes, swizzled) and its
-// MMAs run; completion of the MMAs is tracked with tcgen05.commit on an
-// mbarrier before the planes are overwritten. Accumulators live in TMEM (Re
+// SWIZZLE_128B K-major), eight warps, double-buffered split planes. While the
+// tensor cores run the MMAs of block kb (issued by one thread), all warps
+// load block kb+1 from global memory into registers, wait for the MMAs of
+// block kb-1 to release the other plane buffer (tcgen05.commit -> mbarrier),
+// then split and store it swizzled. Accumulators live in TMEM (Re
 // in columns 0-63, Im in 64-127) and are read back with tcgen05.ld for the
 // fused epilogue. Every mbarrier wait is bounded; on a time-out the CTA
 // raises the error flag, skips its epilogue, frees its TMEM and returns.
@@ -26,14 +26,13 @@ namespace {
 constexpr int TM = 128;       // UMMA M
 constexpr int TN = 64;        // UMMA N
 constexpr int TK = 32;        // fp32 elements per K block (128 B rows)
-constexpr int THREADS = 128;  // four warps
+constexpr int THREADS = 256;  // eight warps
 constexpr int PLANE_A = TM * TK * 4;  // bytes of one A plane (16 KB)
 constexpr int PLANE_B = TN * TK * 4;  // bytes of one B plane (8 KB)
 constexpr int PLANES_BYTES = 4 * PLANE_A + 4 * PLANE_B;  // re/im x hi/lo for A and B
-constexpr int RAW_A = TM * TK * 8;                           // complex64 tile of op(A), 32 KB
-constexpr int RAW_B = TN * TK * 8;                           // complex64 tile of op(B), 16 KB
-constexpr int RAW_BYTES = RAW_A + RAW_B;
-constexpr int RAW_STAGES = 2;
+constexpr int STAGES = 2;                                    // double-buffered planes
+constexpr int A_TASKS = TM * (TK / 4) / THREADS;             // 4 row-chunks of op(A) per thread
+constexpr int B_TASKS = TN * (TK / 4) / THREADS;             // 2 row-chunks of op(B) per thread
 constexpr int TMEM_COLS = 128;
 constexpr long long kWaitLimit = 1ll << 26;  // bounded mbarrier polls
 
@@ -133,51 +132,75 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
-  const int bytes = pred ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_addr(smem)), "l"(gmem),
-               "r"(bytes));
+struct Regs {
+  float2 a[A_TASKS][4];
+  float2 b[B_TASKS][4];
+};
+
+// Task t of op(A): (row, chunk of 4 k). Lanes walk the memory-contiguous index.
+template <int OPA>
+__device__ __forceinline__ void a_task(int t, int& row, int& chunk) {
+  if (OPA == 0) {
+    row = t >> 3;
+    chunk = t & 7;
+  } else {
+    row = t & (TM - 1);
+    chunk = t >> 7;
+  }
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+template <int OPB>
+__device__ __forceinline__ void b_task(int t, int& row, int& chunk) {
+  if (OPB == 1) {
+    row = t >> 3;
+    chunk = t & 7;
+  } else {
+    row = t & (TN - 1);
+    chunk = t >> 6;
+  }
 }
 
-// Raw staging of one K block in the operands' memory order:
-//   op(A) = A   : rawA[r][k] (128 x 32);   op(A) = A^H : rawA[k][r] (32 x 128)
-//   op(B) = B   : rawB[k][n] (32 x 64);    op(B) = B^H : rawB[n][k] (64 x 32)
+// Global -> registers for one K block (all loads issued back to back).
 template <int OPA, int OPB>
-__device__ __forceinline__ void load_raw(const Args& a, const c32* Ag, const c32* Bg, uint8_t* raw,
-                                         int m0, int n0, int k0, int tid) {
-  c32* ra = reinterpret_cast<c32*>(raw);
-  c32* rb = reinterpret_cast<c32*>(raw + RAW_A);
-#pragma unroll 4
-  for (int t = tid; t < TM * TK; t += THREADS) {
-    if (OPA == 0) {
-      const int r = t >> 5, k = t & 31;  // consecutive threads walk k
-      const int gr = m0 + r, gk = k0 + k;
-      const bool ok = gr < a.M && gk < a.K;
-      cp_async8(ra + r * TK + k, ok ? Ag + (int64_t)gr * a.A.ld + gk : Ag, ok);
-    } else {
-      const int k = t >> 7, r = t & (TM - 1);  // consecutive threads walk r
-      const int gr = m0 + r, gk = k0 + k;
-      const bool ok = gr < a.M && gk < a.K;
-      cp_async8(ra + k * TM + r, ok ? Ag + (int64_t)gk * a.A.ld + gr : Ag, ok);
+__device__ __forceinline__ void load_regs(const Args& a, const c32* Ag, const c32* Bg, Regs& R, int m0,
+                                          int n0, int k0, int tid) {
+#pragma unroll
+  for (int i = 0; i < A_TASKS; ++i) {
+    int row, chunk;
+    a_task<OPA>(tid + i * THREADS, row, chunk);
+    const int gr = m0 + row;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = k0 + chunk * 4 + e;
+      float2 v = make_float2(0.f, 0.f);
+      if (gr < a.M && gk < a.K) {
+        if (OPA == 0) {
+          v = Ag[(int64_t)gr * a.A.ld + gk];
+        } else {
+          v = Ag[(int64_t)gk * a.A.ld + gr];
+          v.y = -v.y;
+        }
+      }
+      R.a[i][e] = v;
     }
   }
-#pragma unroll 4
-  for (int t = tid; t < TN * TK; t += THREADS) {
-    if (OPB == 1) {
-      const int n = t >> 5, k = t & 31;
-      const int gn = n0 + n, gk = k0 + k;
-      const bool ok = gn < a.N && gk < a.K;
-      cp_async8(rb + n * TK + k, ok ? Bg + (int64_t)gn * a.B.ld + gk : Bg, ok);
-    } else {
-      const int k = t >> 6, n = t & (TN - 1);
-      const int gn = n0 + n, gk = k0 + k;
-      const bool ok = gn < a.N && gk < a.K;
-      cp_async8(rb + k * TN + n, ok ? Bg + (int64_t)gk * a.B.ld + gn : Bg, ok);
+#pragma unroll
+  for (int i = 0; i < B_TASKS; ++i) {
+    int row, chunk;
+    b_task<OPB>(tid + i * THREADS, row, chunk);
+    const int gn = n0 + row;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = k0 + chunk * 4 + e;
+      float2 v = make_float2(0.f, 0.f);
+      if (gn < a.N && gk < a.K) {
+        if (OPB == 0) {
+          v = Bg[(int64_t)gk * a.B.ld + gn];
+        } else {
+          v = Bg[(int64_t)gn * a.B.ld + gk];
+          v.y = -v.y;
+        }
+      }
+      R.b[i][e] = v;
     }
   }
 }
@@ -197,59 +220,28 @@ __device__ __forceinline__ void split4(const float2 (&v)[4], float4& hr, float4&
   }
 }
 
-// Raw tiles -> the eight split planes (SWIZZLE_128B K-major), conjugating
-// the transposed operands.
+// Registers -> the eight split planes (SWIZZLE_128B K-major).
 template <int OPA, int OPB>
-__device__ __forceinline__ void convert_raw(const uint8_t* raw, uint8_t* planes, int tid) {
-  const c32* ra = reinterpret_cast<const c32*>(raw);
-  const c32* rb = reinterpret_cast<const c32*>(raw + RAW_A);
+__device__ __forceinline__ void store_planes(const Regs& R, uint8_t* planes, int tid) {
   uint8_t* pb = planes + 4 * PLANE_A;
-#pragma unroll 2
-  for (int t = tid; t < TM * (TK / 4); t += THREADS) {
+#pragma unroll
+  for (int i = 0; i < A_TASKS; ++i) {
     int row, chunk;
-    float2 v[4];
-    if (OPA == 0) {
-      row = t >> 3;
-      chunk = t & 7;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = ra[row * TK + chunk * 4 + e];
-    } else {
-      row = t & (TM - 1);
-      chunk = t >> 7;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        v[e] = ra[(chunk * 4 + e) * TM + row];
-        v[e].y = -v[e].y;
-      }
-    }
+    a_task<OPA>(tid + i * THREADS, row, chunk);
     float4 hr, lr, hi, li;
-    split4(v, hr, lr, hi, li);
+    split4(R.a[i], hr, lr, hi, li);
     const uint32_t off = sw128_offset(row, chunk);
     *reinterpret_cast<float4*>(planes + off) = hr;
     *reinterpret_cast<float4*>(planes + PLANE_A + off) = lr;
     *reinterpret_cast<float4*>(planes + 2 * PLANE_A + off) = hi;
     *reinterpret_cast<float4*>(planes + 3 * PLANE_A + off) = li;
   }
-#pragma unroll 2
-  for (int t = tid; t < TN * (TK / 4); t += THREADS) {
+#pragma unroll
+  for (int i = 0; i < B_TASKS; ++i) {
     int row, chunk;
-    float2 v[4];
-    if (OPB == 1) {
-      row = t >> 3;
-      chunk = t & 7;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        v[e] = rb[row * TK + chunk * 4 + e];
-        v[e].y = -v[e].y;
-      }
-    } else {
-      row = t & (TN - 1);
-      chunk = t >> 6;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = rb[(chunk * 4 + e) * TN + row];
-    }
+    b_task<OPB>(tid + i * THREADS, row, chunk);
     float4 hr, lr, hi, li;
-    split4(v, hr, lr, hi, li);
+    split4(R.b[i], hr, lr, hi, li);
     const uint32_t off = sw128_offset(row, chunk);
     *reinterpret_cast<float4*>(pb + off) = hr;
     *reinterpret_cast<float4*>(pb + PLANE_B + off) = lr;
@@ -289,10 +281,9 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the SWIZZLE_128B atoms.
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* planes = smem;
-  uint8_t* raw = smem + PLANES_BYTES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(raw + RAW_STAGES * RAW_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  uint8_t* planes = smem;  // STAGES x PLANES_BYTES
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * PLANES_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + STAGES);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -308,56 +299,60 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    mbar_init(bar, 1);
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
-  uint32_t phase = 0;
+  uint32_t phase[STAGES] = {0, 0};
   bool ok = true;
+  Regs R;
 
   for (int64_t b = blockIdx.z; b < a.batch && ok; b += gridDim.z) {
     const c32* Ag = at<const c32>(a.A, b);
     const c32* Bg = at<const c32>(a.B, b);
-    // Prologue: raw tiles of blocks 0 and 1 in flight.
-    for (int s = 0; s < RAW_STAGES; ++s) {
-      if (s < KB) load_raw<OPA, OPB>(a, Ag, Bg, raw + s * RAW_BYTES, m0, n0, s * TK, tid);
-      cp_async_commit();
-    }
-    for (int kb = 0; kb < KB; ++kb) {
-      cp_async_wait<RAW_STAGES - 1>();  // block kb has landed
-      __syncthreads();
-      if (kb > 0) {  // the planes are still being read by the MMAs of block kb - 1
-        if (!mbar_wait(bar, phase)) ok = false;
-        phase ^= 1u;
-      }
-      if (ok) convert_raw<OPA, OPB>(raw + (kb % RAW_STAGES) * RAW_BYTES, planes, tid);
+    if (KB > 0) {
+      load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, 0, tid);
+      store_planes<OPA, OPB>(R, planes, tid);
       fence_async_smem();
       __syncthreads();
-      // The raw slot of block kb is free again: fetch block kb + 2 into it.
-      if (kb + RAW_STAGES < KB && ok)
-        load_raw<OPA, OPB>(a, Ag, Bg, raw + (kb % RAW_STAGES) * RAW_BYTES, m0, n0, (kb + RAW_STAGES) * TK,
-                           tid);
-      cp_async_commit();
-      if (tid == 0 && ok) {
+    }
+    for (int kb = 0; kb < KB; ++kb) {
+      const int s = kb % STAGES;
+      if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-        const uint32_t sa = smem_addr(planes);
+        const uint32_t sa = smem_addr(planes + s * PLANES_BYTES);
         const uint32_t sb = sa + 4 * PLANE_A;
 #pragma unroll
         for (int kk = 0; kk < TK / 8; ++kk) issue_kstep(tmem, sa, sb, kk, kb == 0 && kk == 0);
-        mma_commit(bar);
+        mma_commit(&bars[s]);
+      }
+      if (kb + 1 < KB) {
+        const int s1 = (kb + 1) % STAGES;
+        load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
+        if (kb >= 1) {  // buffer s1 was read by the MMAs of block kb - 1
+          if (!mbar_wait(&bars[s1], phase[s1])) ok = false;
+          phase[s1] ^= 1u;
+        }
+        if (ok) store_planes<OPA, OPB>(R, planes + s1 * PLANES_BYTES, tid);
+        fence_async_smem();
       }
       if (!__syncthreads_and(ok)) {
         ok = false;
         break;
       }
     }
-    cp_async_wait<0>();
     if (KB > 0 && ok) {
-      if (!mbar_wait(bar, phase)) ok = false;
-      phase ^= 1u;
+      if (KB >= 2) {
+        const int sp = (KB - 2) % STAGES;
+        if (!mbar_wait(&bars[sp], phase[sp])) ok = false;
+        phase[sp] ^= 1u;
+      }
+      const int sl = (KB - 1) % STAGES;
+      if (!mbar_wait(&bars[sl], phase[sl])) ok = false;
+      phase[sl] ^= 1u;
     }
     if (!__syncthreads_and(ok)) {
       ok = false;
@@ -365,11 +360,13 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
 
-    // Epilogue: warp w owns TMEM lanes 32w..32w+31 = tile rows.
-    const int r = m0 + warp * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (= tile rows);
+    // warps 0-3 take columns 0-31, warps 4-7 columns 32-63.
+    const int wl = warp & 3;
+    const int r = m0 + wl * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
 #pragma unroll 1
-    for (int c0 = 0; c0 < TN; c0 += 16) {
+    for (int c0 = (warp >> 2) * (TN / 2); c0 < (warp >> 2) * (TN / 2) + TN / 2; c0 += 16) {
       uint32_t vr[16], vi[16];
       if (KB > 0) {
         asm volatile(
@@ -434,7 +431,7 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
 
 template <int OPA, int OPB>
 int launch(const Args& a, cudaStream_t s) {
-  const size_t smem = (size_t)PLANES_BYTES + (size_t)RAW_STAGES * RAW_BYTES + 64 + 1024;
+  const size_t smem = (size_t)STAGES * PLANES_BYTES + 64 + 1024;
   QTX_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<OPA, OPB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((a.N + TN - 1) / TN, (a.M + TM - 1) / TM, (unsigned)(a.batch < 65535 ? a.batch : 65535));
