@@ -10,14 +10,18 @@
 // negate bit: 12 tcgen05.mma.kind::tf32 per K step of 8.
 //
 // CTA tile 128 x 64 (one UMMA M=128, N=64), K block 32 FP32 (128-byte rows,
-// SWIZZLE_128B K-major), eight warps, double-buffered split planes. While the
-// tensor cores run the MMAs of block kb (issued by one thread), all warps
-// load block kb+1 from global memory into registers, wait for the MMAs of
-// block kb-1 to release the other plane buffer (tcgen05.commit -> mbarrier),
-// then split and store it swizzled. Accumulators live in TMEM (Re
-// in columns 0-63, Im in 64-127) and are read back with tcgen05.ld for the
-// fused epilogue. Every mbarrier wait is bounded; on a time-out the CTA
-// raises the error flag, skips its epilogue, frees its TMEM and returns.
+// SWIZZLE_128B K-major), eight warps, one buffer of split planes (96 KB) so
+// that two CTAs share an SM and one's prologue/epilogue overlaps the other's
+// MMAs. While the tensor cores run the MMAs of block kb (issued by one
+// thread), all warps load block kb+1 from global memory into registers, wait
+// for the MMAs (tcgen05.commit -> mbarrier), then split and store the planes.
+// Accumulators live in TMEM (Re in columns 0-63, Im in 64-127) and are read
+// back with tcgen05.ld. The epilogue goes through a padded shared-memory tile
+// so that global reads and writes are coalesced in either orientation:
+// row-per-lane for conjugate-transposed addends and the transposed store,
+// column-per-lane for everything else. Every mbarrier wait is bounded; on a
+// time-out the CTA raises the error flag, skips its epilogue, frees its TMEM
+// and returns.
 #include "common.cuh"
 
 namespace qtx {
@@ -30,7 +34,8 @@ constexpr int THREADS = 256;  // eight warps
 constexpr int PLANE_A = TM * TK * 4;  // bytes of one A plane (16 KB)
 constexpr int PLANE_B = TN * TK * 4;  // bytes of one B plane (8 KB)
 constexpr int PLANES_BYTES = 4 * PLANE_A + 4 * PLANE_B;  // re/im x hi/lo for A and B
-constexpr int STAGES = 2;                                    // double-buffered planes
+constexpr int CTAS_PER_SM = 2;                               // one plane buffer each
+constexpr int S_LD = TN + 1;                                 // padded epilogue tile row (float2)
 constexpr int A_TASKS = TM * (TK / 4) / THREADS;             // 4 row-chunks of op(A) per thread
 constexpr int B_TASKS = TN * (TK / 4) / THREADS;             // 2 row-chunks of op(B) per thread
 constexpr int TMEM_COLS = 128;
@@ -276,14 +281,23 @@ __device__ __forceinline__ void issue_kstep(uint32_t tmem, uint32_t sa, uint32_t
   mma_tf32(im, aih, brh, ID, 1u);
 }
 
+__device__ __forceinline__ float2 addend_at(const Args& a, int t, int64_t b, int r, int c) {
+  const auto& ad = a.add[t];
+  const c32* p = at<const c32>(ad.m, b);
+  float2 x = ad.ct ? p[(int64_t)c * ad.m.ld + r] : p[(int64_t)r * ad.m.ld + c];
+  if (ad.ct) x.y = -x.y;
+  return cmulf(ad.coef, x);
+}
+
 template <int OPA, int OPB>
-__global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Args a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the SWIZZLE_128B atoms.
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* planes = smem;  // STAGES x PLANES_BYTES
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * PLANES_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + STAGES);
+  uint8_t* planes = smem;
+  float2* tile = reinterpret_cast<float2*>(smem);  // epilogue tile [TM][S_LD], reuses the planes
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + PLANES_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -299,16 +313,20 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
-  uint32_t phase[STAGES] = {0, 0};
+  uint32_t phase = 0;
   bool ok = true;
   Regs R;
+  // Addends split by orientation: conjugate-transposed ones are read with
+  // lanes along rows (phase A), the others with lanes along columns (phase B).
+  int n_ct = 0;
+  for (int t = 0; t < a.nadd; ++t) n_ct += a.add[t].ct;
 
   for (int64_t b = blockIdx.z; b < a.batch && ok; b += gridDim.z) {
     const c32* Ag = at<const c32>(a.A, b);
@@ -320,23 +338,20 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
       __syncthreads();
     }
     for (int kb = 0; kb < KB; ++kb) {
-      const int s = kb % STAGES;
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-        const uint32_t sa = smem_addr(planes + s * PLANES_BYTES);
+        const uint32_t sa = smem_addr(planes);
         const uint32_t sb = sa + 4 * PLANE_A;
 #pragma unroll
         for (int kk = 0; kk < TK / 8; ++kk) issue_kstep(tmem, sa, sb, kk, kb == 0 && kk == 0);
-        mma_commit(&bars[s]);
+        mma_commit(bar);
       }
-      if (kb + 1 < KB) {
-        const int s1 = (kb + 1) % STAGES;
-        load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
-        if (kb >= 1) {  // buffer s1 was read by the MMAs of block kb - 1
-          if (!mbar_wait(&bars[s1], phase[s1])) ok = false;
-          phase[s1] ^= 1u;
-        }
-        if (ok) store_planes<OPA, OPB>(R, planes + s1 * PLANES_BYTES, tid);
+      const bool more = kb + 1 < KB;
+      if (more) load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
+      if (!mbar_wait(bar, phase)) ok = false;
+      phase ^= 1u;
+      if (more && ok) {
+        store_planes<OPA, OPB>(R, planes, tid);
         fence_async_smem();
       }
       if (!__syncthreads_and(ok)) {
@@ -344,83 +359,95 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
         break;
       }
     }
-    if (KB > 0 && ok) {
-      if (KB >= 2) {
-        const int sp = (KB - 2) % STAGES;
-        if (!mbar_wait(&bars[sp], phase[sp])) ok = false;
-        phase[sp] ^= 1u;
-      }
-      const int sl = (KB - 1) % STAGES;
-      if (!mbar_wait(&bars[sl], phase[sl])) ok = false;
-      phase[sl] ^= 1u;
-    }
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
+    if (!ok) break;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
 
-    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (= tile rows);
-    // warps 0-3 take columns 0-31, warps 4-7 columns 32-63.
-    const int wl = warp & 3;
-    const int r = m0 + wl * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+    // Phase A (warps 0-3 and 4-7 split the columns; lane = tile row, the
+    // TMEM lane quarter of warp w is w % 4): alpha * acc + ct addends -> tile.
+    {
+      const int wl = warp & 3;
+      const int rl = wl * 32 + lane;
+      const int r = m0 + rl;
+      const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+      const int cbeg = (warp >> 2) * (TN / 2);
 #pragma unroll 1
-    for (int c0 = (warp >> 2) * (TN / 2); c0 < (warp >> 2) * (TN / 2) + TN / 2; c0 += 16) {
-      uint32_t vr[16], vi[16];
-      if (KB > 0) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]),
-              "=r"(vr[6]), "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]),
-              "=r"(vr[12]), "=r"(vr[13]), "=r"(vr[14]), "=r"(vr[15])
-            : "r"(lane_base + (uint32_t)c0));
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]),
-              "=r"(vi[6]), "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]),
-              "=r"(vi[12]), "=r"(vi[13]), "=r"(vi[14]), "=r"(vi[15])
-            : "r"(lane_base + (uint32_t)(TN + c0)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-      } else {
+      for (int c0 = cbeg; c0 < cbeg + TN / 2; c0 += 16) {
+        uint32_t vr[16], vi[16];
+        if (KB > 0) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+              : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]),
+                "=r"(vr[6]), "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]),
+                "=r"(vr[12]), "=r"(vr[13]), "=r"(vr[14]), "=r"(vr[15])
+              : "r"(lane_base + (uint32_t)c0));
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+              : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]),
+                "=r"(vi[6]), "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]),
+                "=r"(vi[12]), "=r"(vi[13]), "=r"(vi[14]), "=r"(vi[15])
+              : "r"(lane_base + (uint32_t)(TN + c0)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0u;
-      }
-      if (r < a.M) {
+          for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0u;
+        }
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int c = n0 + c0 + j;
-          if (c >= a.N) continue;
           float2 v = cmulf(a.alpha, make_float2(__uint_as_float(vr[j]), __uint_as_float(vi[j])));
-          for (int t = 0; t < a.nadd; ++t) {
-            const auto& ad = a.add[t];
-            const c32* p = at<const c32>(ad.m, b);
-            float2 x = ad.ct ? p[(int64_t)c * ad.m.ld + r] : p[(int64_t)r * ad.m.ld + c];
-            if (ad.ct) x.y = -x.y;
-            const float2 y = cmulf(ad.coef, x);
-            v.x += y.x;
-            v.y += y.y;
-          }
-          if (!a.C3.null()) {
-            float2 v3 = cmulf(a.scale3, v);
-            for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) {
-              const auto& ad = a.add[t];
-              const c32* p = at<const c32>(ad.m, b);
-              float2 x = ad.ct ? p[(int64_t)c * ad.m.ld + r] : p[(int64_t)r * ad.m.ld + c];
-              if (ad.ct) x.y = -x.y;
-              const float2 y = cmulf(ad.coef, x);
-              v3.x += y.x;
-              v3.y += y.y;
+          if (n_ct > 0 && r < a.M && c < a.N) {
+            for (int t = 0; t < a.nadd; ++t) {
+              if (!a.add[t].ct) continue;
+              const float2 y = addend_at(a, t, b, r, c);
+              v.x += y.x;
+              v.y += y.y;
             }
-            at<c32>(a.C3, b)[(int64_t)r * a.C3.ld + c] = v3;
           }
-          if (!a.C2.null())
-            at<c32>(a.C2, b)[(int64_t)c * a.C2.ld + r] = cmulf(a.coef2, make_float2(v.x, -v.y));
-          if (!a.C.null()) at<c32>(a.C, b)[(int64_t)r * a.C.ld + c] = v;
+          tile[rl * S_LD + c0 + j] = v;
         }
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+
+    // Phase B (lane = tile column): remaining addends, C3 and C.
+#pragma unroll 1
+    for (int e = tid; e < TM * TN; e += THREADS) {
+      const int rl = e / TN, cl = e % TN;
+      const int r = m0 + rl, c = n0 + cl;
+      if (r >= a.M || c >= a.N) continue;
+      float2 v = tile[rl * S_LD + cl];
+      for (int t = 0; t < a.nadd; ++t) {
+        if (a.add[t].ct) continue;
+        const float2 y = addend_at(a, t, b, r, c);
+        v.x += y.x;
+        v.y += y.y;
+      }
+      if (!a.C3.null()) {
+        float2 v3 = cmulf(a.scale3, v);
+        for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) {
+          const float2 y = addend_at(a, t, b, r, c);
+          v3.x += y.x;
+          v3.y += y.y;
+        }
+        at<c32>(a.C3, b)[(int64_t)r * a.C3.ld + c] = v3;
+      }
+      if (!a.C.null()) at<c32>(a.C, b)[(int64_t)r * a.C.ld + c] = v;
+      if (!a.C2.null()) tile[rl * S_LD + cl] = v;
+    }
+
+    // Phase C (lane = tile row): the conjugate-transposed store C2.
+    if (!a.C2.null()) {
+      __syncthreads();
+#pragma unroll 1
+      for (int e = tid; e < TM * TN; e += THREADS) {
+        const int rl = e % TM, cl = e / TM;
+        const int r = m0 + rl, c = n0 + cl;
+        if (r >= a.M || c >= a.N) continue;
+        const float2 v = tile[rl * S_LD + cl];
+        at<c32>(a.C2, b)[(int64_t)c * a.C2.ld + r] = cmulf(a.coef2, make_float2(v.x, -v.y));
+      }
+    }
     __syncthreads();
   }
   if (!ok && tid == 0 && a.err != nullptr) atomicExch(a.err, 1);
@@ -431,7 +458,8 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tc_kernel(const Args a) {
 
 template <int OPA, int OPB>
 int launch(const Args& a, cudaStream_t s) {
-  const size_t smem = (size_t)STAGES * PLANES_BYTES + 64 + 1024;
+  static_assert(TM * S_LD * (int)sizeof(float2) <= PLANES_BYTES, "epilogue tile must fit the planes");
+  const size_t smem = (size_t)PLANES_BYTES + 64 + 1024;
   QTX_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<OPA, OPB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((a.N + TN - 1) / TN, (a.M + TM - 1) / TM, (unsigned)(a.batch < 65535 ? a.batch : 65535));
