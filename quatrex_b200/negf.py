@@ -35,7 +35,7 @@ from . import _native
 from ._interop import mat
 from ._native import NULL_MAT, QtxBT, QtxMat
 from .obc import SanchoRubio, fixed_point_refine
-from .utils import workspace_pool
+from .utils import WorkspacePool
 
 _C128 = torch.complex128
 
@@ -87,12 +87,18 @@ class EnergyPointSolver:
         and runs its products on tcgen05 as split-TF32 products with FP32
         accumulation, inverting every Schur complement in FP64; the
         transmission is formed in FP64 from the complex64 corner block.
+    store_blocks : bool
+        True (default): the G^<, G^> (diagonal and off-diagonal) and G^R
+        diagonal blocks of the last batch are kept in ``PointResult.blocks``.
+        False: only the observables (transmission, density, current) are
+        produced; the solve writes no output blocks, which roughly halves the
+        device memory per energy.
     """
 
     def __init__(self, h_diag, coupling, eta: float = 1e-4, sr_tol: float = 1e-12,
                  sr_max_iterations: int = 100, per_energy: bool = True,
                  skip_zero_scattering: bool = False, device: torch.device | None = None,
-                 precision: str = "fp64", device_loop: bool = False):
+                 precision: str = "fp64", device_loop: bool = False, store_blocks: bool = True):
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -113,13 +119,22 @@ class EnergyPointSolver:
                               per_energy=per_energy)
         self.skip_zero_scattering = skip_zero_scattering
         self.device_loop = device_loop
+        self.store_blocks = store_blocks
         self._bufs: dict = {}
         self._graphs: dict = {}
         self._host_sr = (0, True)
         self._last_device_loop = device_loop
+        # Workspaces belong to this solver: captured graphs hold their
+        # addresses, and solvers on concurrent streams must not share them.
+        self._ws = WorkspacePool()
         self.lib = _native.load()
 
     # ------------------------------------------------------------------
+    def resident_bytes(self, B: int) -> int:
+        """Device bytes this solver holds for batch size B (buffers and
+        workspaces), without allocating anything."""
+        return resident_bytes(self.N, self.b, B, self.precision, self.lib, self.store_blocks)
+
     def _buffers(self, B: int) -> dict:
         buf = self._bufs.get(B)
         if buf is not None:
@@ -128,10 +143,14 @@ class EnergyPointSolver:
         z = lambda *s: torch.empty(s, dtype=_C128, device=dev)  # noqa: E731
         ot = torch.complex64 if self.precision == "mixed" else _C128
         o = lambda *s: torch.empty(s, dtype=ot, device=dev)  # noqa: E731
+        n1 = max(N - 1, 1)
+        if self.store_blocks:
+            outs = dict(xl_d=o(N, B, b, b), xl_u=o(n1, B, b, b), xl_l=o(n1, B, b, b), xg_d=o(N, B, b, b),
+                        xg_u=o(n1, B, b, b), xg_l=o(n1, B, b, b), xr_d=o(N, B, b, b))
+        else:
+            outs = {}
         buf = dict(
-            a_diag=z(N, B, b, b), xl_d=o(N, B, b, b), xl_u=o(max(N - 1, 1), B, b, b),
-            xl_l=o(max(N - 1, 1), B, b, b), xg_d=o(N, B, b, b), xg_u=o(max(N - 1, 1), B, b, b),
-            xg_l=o(max(N - 1, 1), B, b, b), xr_d=o(N, B, b, b), g0n=o(B, b, b),
+            a_diag=z(N, B, b, b), g0n=o(B, b, b), **outs,
             gl=z(B, b, b), gr=z(B, b, b), sig=[z(B, b, b) for _ in range(6)],
             current=z(B, N + 1), density=torch.empty((B, N * b), dtype=torch.float64, device=dev),
             T=torch.empty(B, dtype=torch.float64, device=dev), zE=z(B),
@@ -183,6 +202,16 @@ class EnergyPointSolver:
         buf["fr"].copy_(torch.as_tensor(np.asarray(f_right, dtype=np.float64)).reshape(-1))
         return B
 
+    def set_inputs_device(self, energies: torch.Tensor, f_left: torch.Tensor, f_right: torch.Tensor) -> int:
+        """set_inputs() from device tensors: asynchronous copies on the
+        current stream (no host synchronisation)."""
+        B = int(energies.numel())
+        buf = self._buffers(B)
+        buf["E"].copy_(energies.reshape(-1), non_blocking=True)
+        buf["fl"].copy_(f_left.reshape(-1), non_blocking=True)
+        buf["fr"].copy_(f_right.reshape(-1), non_blocking=True)
+        return B
+
     def capture(self, B: int) -> "torch.cuda.CUDAGraph":
         """Captures the whole energy-point pipeline for batch size B in one
         CUDA graph (Sancho-Rubio runs its device-side convergence loop). The
@@ -220,8 +249,11 @@ class EnergyPointSolver:
     def _result(self, B: int) -> PointResult:
         buf = self._bufs[B]
         sig = buf["sig"]
-        blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
-                      xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
+        if self.store_blocks:
+            blocks = dict(xl_diag=buf["xl_d"], xl_upper=buf["xl_u"], xl_lower=buf["xl_l"], xg_diag=buf["xg_d"],
+                          xg_upper=buf["xg_u"], xg_lower=buf["xg_l"], xr_diag=buf["xr_d"], g0n=buf["g0n"])
+        else:
+            blocks = dict(g0n=buf["g0n"])
         its = (self._host_sr[0],) * 2 if not self._last_device_loop else ("device", "device")
         return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], its, blocks)
 
@@ -252,7 +284,7 @@ class EnergyPointSolver:
                  (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))
         self._sr_both(sides, B, stream, device_loop, buf)
         for k, (aii, aij, aji, g, f, s3) in enumerate(sides):
-            ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
+            ws = self._ws.get(lib.qtx_obc_workspace(b, B), dev, "obc")
             _native.check(lib.qtx_obc_refine(b, B, mat(aii), aij, aji, mat(g), mat(g),
                                              buf["res_rel"][k].data_ptr(), buf["res_abs"][k].data_ptr(), None,
                                              ws.data_ptr(), ws.numel(), stream))
@@ -279,11 +311,17 @@ class EnergyPointSolver:
         A = self._bt([mat(ad[i]) for i in range(N)], [up_s] * (N - 1), [lo_s] * (N - 1), keep)
         zs = NULL_MAT if self.skip_zero_scattering else _bcast(zero)
         S = self._bt([zs] * N, [zs] * (N - 1), [zs] * (N - 1), keep)
-        XL = self._bt([mat(buf["xl_d"][i]) for i in range(N)], [mat(buf["xl_u"][i]) for i in range(N - 1)],
-                      [mat(buf["xl_l"][i]) for i in range(N - 1)], keep)
-        XG = self._bt([mat(buf["xg_d"][i]) for i in range(N)], [mat(buf["xg_u"][i]) for i in range(N - 1)],
-                      [mat(buf["xg_l"][i]) for i in range(N - 1)], keep)
-        XR = self._bt([mat(buf["xr_d"][i]) for i in range(N)], [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1), keep)
+        if self.store_blocks:
+            XL = self._bt([mat(buf["xl_d"][i]) for i in range(N)], [mat(buf["xl_u"][i]) for i in range(N - 1)],
+                          [mat(buf["xl_l"][i]) for i in range(N - 1)], keep)
+            XG = self._bt([mat(buf["xg_d"][i]) for i in range(N)], [mat(buf["xg_u"][i]) for i in range(N - 1)],
+                          [mat(buf["xg_l"][i]) for i in range(N - 1)], keep)
+            XR = self._bt([mat(buf["xr_d"][i]) for i in range(N)], [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1),
+                          keep)
+        else:  # observables only: the solve keeps its blocks in its workspace
+            XL = self._bt([NULL_MAT] * N, [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1), keep)
+            XG = self._bt([NULL_MAT] * N, [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1), keep)
+            XR = self._bt([NULL_MAT] * N, [NULL_MAT] * (N - 1), [NULL_MAT] * (N - 1), keep)
         obc = []
         for k in range(3):
             arr = (QtxMat * N)(*([NULL_MAT] * N))
@@ -292,7 +330,7 @@ class EnergyPointSolver:
             obc.append(arr)
         wsq = lib.qtx_selected_solve_mixed_workspace if mixed else lib.qtx_selected_solve_workspace
         solve = lib.qtx_selected_solve_mixed if mixed else lib.qtx_selected_solve
-        ws = workspace_pool.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
+        ws = self._ws.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
         _native.check(solve(
             ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
             ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
@@ -304,7 +342,7 @@ class EnergyPointSolver:
             _native.check(lib.qtx_convert(b, b, B, mat(g0n), _native.QTX_C64, mat(buf["g0n128"]),
                                           _native.QTX_C128, stream))
             g0n = buf["g0n128"]
-        ws = workspace_pool.get(lib.qtx_obc_workspace(b, B), dev, "obc")
+        ws = self._ws.get(lib.qtx_obc_workspace(b, B), dev, "obc")
         _native.check(lib.qtx_transmission(b, b, B, mat(g0n), mat(sig[0]), mat(sig[3]),
                                            buf["T"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
         return self._result(B)
@@ -312,7 +350,7 @@ class EnergyPointSolver:
     def _sr_both(self, sides, B: int, stream, device_loop: bool, buf):
         """Both contacts' Sancho-Rubio in one decimation loop (2B entries)."""
         lib, dev = self.lib, self.device
-        ws = workspace_pool.get(lib.qtx_sancho_rubio_workspace(self.b, 2 * B), dev, "sr")
+        ws = self._ws.get(lib.qtx_sancho_rubio_workspace(self.b, 2 * B), dev, "sr")
         batches = (ctypes.c_int64 * 2)(B, B)
         aii = (QtxMat * 2)(mat(sides[0][0]), mat(sides[1][0]))
         aij = (QtxMat * 2)(sides[0][1], sides[1][1])
@@ -330,6 +368,26 @@ class EnergyPointSolver:
             int(self.sr.per_energy), ctypes.byref(it), ctypes.byref(conv), None, ws.data_ptr(), ws.numel(),
             stream))
         self._host_sr = (it.value, bool(conv.value))
+
+
+def resident_bytes(N: int, b: int, B: int, precision: str = "fp64", lib=None, store_blocks: bool = True) -> int:
+    """Device bytes of an EnergyPointSolver(N blocks of b x b) at batch size
+    B: the block stacks of EnergyPointSolver._buffers plus the selected-solve,
+    Sancho-Rubio and OBC workspaces (sizes from the library's own queries)."""
+    lib = lib or _native.load()
+    bb = b * b
+    n1 = max(N - 1, 1)
+    osz = 8 if precision == "mixed" else 16
+    total = 16 * (N * B * bb + 2 * B * bb + 6 * B * bb + B * (N + 1) + B)  # a_diag, g, sigma, current, zE
+    total += 8 * (B * N * b + 5 * B) + 4 * (B + 2)  # density, T/E/fl/fr, info, SR status
+    total += 16 * 2 * B  # residual vectors
+    total += osz * ((3 * N + 4 * n1) * B * bb if store_blocks else 0) + osz * B * bb  # output blocks, corner
+    if precision == "mixed":
+        total += 8 * (N * B * bb + 6 * B * bb) + 16 * B * bb
+    bs = (ctypes.c_int32 * N)(*([b] * N))
+    wsq = lib.qtx_selected_solve_mixed_workspace if precision == "mixed" else lib.qtx_selected_solve_workspace
+    total += int(wsq(N, bs, B, 1)) + int(lib.qtx_sancho_rubio_workspace(b, 2 * B)) + int(lib.qtx_obc_workspace(b, B))
+    return int(total)
 
 
 def flops_per_energy(N: int, b: int, sr_iterations: tuple = (0, 0)) -> dict:
