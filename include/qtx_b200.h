@@ -106,6 +106,23 @@ int qtx_cgemm_batched(int m, int n, int k, int64_t batch, float alpha_re, float 
  * column of a zero pivot (may be NULL). X may equal A. */
 int qtx_zinv_batched(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, qtx_stream stream);
 
+/* Scratch bytes of qtx_zinv_batched_ws. */
+size_t qtx_zinv_workspace(int n, int64_t batch);
+
+/* qtx_zinv_batched with scratch: for large blocks and small batches the
+ * inverse runs as a multi-CTA blocked Gauss-Jordan (panel factorisation,
+ * row interchanges, DMMA trailing update over every SM), otherwise as one CTA
+ * per matrix. Same pivot rule and info convention. The library's RGF and
+ * Sancho-Rubio drivers invert through this path. Replaces the same
+ * qttools/kernels/linalg/inv.py:6-40 call as qtx_zinv_batched. */
+int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, void* workspace,
+                        size_t workspace_bytes, qtx_stream stream);
+
+/* Inverse path of every workspace-backed inverse in this process: 0
+ * automatic (default), 1 one CTA per matrix, 2 multi-CTA. A tuning and test
+ * knob; no reference counterpart. */
+int qtx_set_inverse_path(int mode);
+
 /* Workspace bytes for qtx_selected_inv on this block layout and batch. */
 size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch);
 

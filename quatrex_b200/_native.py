@@ -53,6 +53,9 @@ SIGNATURES = {
                                   QtxMat, c_int, ctypes.c_float, ctypes.c_float, QtxMat, c_int, QtxMat, c_void_p,
                                   c_void_p]),
     "qtx_zinv_batched": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p]),
+    "qtx_zinv_workspace": (c_size_t, [c_int, c_int64]),
+    "qtx_zinv_batched_ws": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "qtx_set_inverse_path": (c_int, [c_int]),
     "qtx_selected_inv_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64]),
     "qtx_selected_inv": (c_int, [POINTER(QtxBT), POINTER(QtxMat), POINTER(QtxBT), c_int64, c_void_p,
                                  c_void_p, c_size_t, c_void_p]),

@@ -136,6 +136,7 @@ size_t inv_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch) {
   for (int i = 0; i < nb; ++i) bm = bs[i] > bm ? bs[i] : bm;
   for (int i = 0; i < nb; ++i) ws.mat(bs[i], bs[i], batch);
   for (int k = 0; k < 6; ++k) ws.mat(bm, bm, batch);
+  ws.take(zinv_scratch_bytes(bm, batch));
   return ws.off + 256;
 }
 
@@ -217,6 +218,30 @@ int qtx_zinv_batched(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, qtx_
     if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, (cudaStream_t)stream));
     return zinv(n, batch, from_abi(a), from_abi(x), info, nullptr, (cudaStream_t)stream);
   });
+}
+
+size_t qtx_zinv_workspace(int n, int64_t batch) { return zinv_scratch_bytes(n, batch) + 256; }
+
+int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, void* workspace,
+                        size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (n < 0 || batch < 0 || a.ptr == nullptr || x.ptr == nullptr) {
+      set_error("qtx_zinv_batched_ws: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, (cudaStream_t)stream));
+    return zinv_ex(n, batch, from_abi(a), from_abi(x), info, nullptr, workspace, workspace_bytes,
+                   (cudaStream_t)stream);
+  });
+}
+
+int qtx_set_inverse_path(int mode) {
+  if (mode < 0 || mode > 2) {
+    set_error("qtx_set_inverse_path: mode must be 0, 1 or 2");
+    return QTX_ERR_ARG;
+  }
+  set_inverse_path(mode);
+  return QTX_OK;
 }
 
 size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch) {

@@ -137,6 +137,14 @@ int cgemm_tc(const CGemmDesc& d, cudaStream_t s);
 // X <- A^{-1} for each of `batch` n x n matrices; X may alias A. `info[b]`
 // (device, optional) receives 0 or the 1-based column of a zero pivot.
 int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s);
+// Inverse with optional scratch (zinv_wide.cu): for large blocks and small
+// batches, a multi-CTA blocked Gauss-Jordan over the whole GPU when
+// `scratch` holds zinv_scratch_bytes(n, batch); otherwise zinv().
+size_t zinv_scratch_bytes(int n, int64_t batch);
+int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, void* scratch,
+            size_t scratch_bytes, cudaStream_t s);
+bool zinv_prefers_wide(int n, int64_t batch);
+void set_inverse_path(int mode);
 
 // Elementwise combination (blockops.cu):
 //   out = sum_t coef_t * op_t(X_t)   for up to 4 terms, over an m x n stack.
@@ -178,9 +186,11 @@ int zre_inner(int m, int n, int64_t batch, MatRef P, MatRef G, double* out, cuda
 int cre_inner(int m, int n, int64_t batch, MatRef P, MatRef G, double* out, cudaStream_t s);
 
 // Launch profiler (profile.cu): RAII bracket of one kernel launch.
+// Scopes nest: only the outermost scope of a thread records, with `launches`
+// kernel launches attributed to it.
 class ProfScope {
  public:
-  ProfScope(int kind, double work, cudaStream_t s);
+  ProfScope(int kind, double work, cudaStream_t s, int launches = 1);
   ~ProfScope();
   ProfScope(const ProfScope&) = delete;
   ProfScope& operator=(const ProfScope&) = delete;

@@ -15,7 +15,10 @@ struct Rec {
   cudaEvent_t a, b;
   int kind;
   double work;
+  int launches;
 };
+
+thread_local int t_depth = 0;
 
 std::mutex g_mu;
 bool g_on = false;
@@ -35,18 +38,20 @@ cudaEvent_t take_event() {
 
 }  // namespace
 
-ProfScope::ProfScope(int kind, double work, cudaStream_t s) : idx_(-1), s_(s) {
+ProfScope::ProfScope(int kind, double work, cudaStream_t s, int launches) : idx_(-1), s_(s) {
+  if (t_depth++ > 0) return;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_on) return;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
-  Rec r{take_event(), take_event(), kind, work};
+  Rec r{take_event(), take_event(), kind, work, launches};
   cudaEventRecord(r.a, s);
   idx_ = (int)g_recs.size();
   g_recs.push_back(r);
 }
 
 ProfScope::~ProfScope() {
+  --t_depth;
   if (idx_ < 0) return;
   std::lock_guard<std::mutex> lk(g_mu);
   if (idx_ < (int)g_recs.size()) cudaEventRecord(g_recs[idx_].b, s_);
@@ -89,7 +94,7 @@ extern "C" int qtx_profile_read(int kind, double* total_ms, double* total_work, 
     }
     ms += t;
     work += r.work;
-    ++n;
+    n += r.launches;
   }
   if (total_ms) *total_ms = ms;
   if (total_work) *total_work = work;

@@ -107,6 +107,8 @@ int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_
   MatRef tP = ws.mat(bm, bm, batch), tU = ws.mat(bm, bm, batch), tT = ws.mat(bm, bm, batch);
   MatRef tXji = ws.mat(bm, bm, batch);
   MatRef tG[2] = {ws.mat(bm, bm, batch), ws.mat(bm, bm, batch)};
+  const size_t scr_bytes = zinv_scratch_bytes(bm, batch);
+  void* scr = ws.take(scr_bytes);
   if (ws.base == nullptr) return QTX_OK;
   if (ws.overflow) {
     set_error("selected_inv: workspace too small");
@@ -118,7 +120,7 @@ int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_
   {
     Addend t[2] = {add(a.diag[0], ONE), add(obc(0), MONE)};
     QTX_TRY(zcombine(bs[0], bs[0], batch, g[0], t, 2, nullptr, s));
-    QTX_TRY(zinv(bs[0], batch, g[0], g[0], info, nullptr, s));
+    QTX_TRY(zinv_ex(bs[0], batch, g[0], g[0], info, nullptr, scr, scr_bytes, s));
   }
   for (int j = 1; j < N; ++j) {
     const int i = j - 1;
@@ -128,7 +130,7 @@ int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_
                 .plus(a.diag[j], ONE)
                 .plus(obc(j), MONE)
                 .run(s));
-    QTX_TRY(zinv(bs[j], batch, g[j], g[j], info, nullptr, s));
+    QTX_TRY(zinv_ex(bs[j], batch, g[j], g[j], info, nullptr, scr, scr_bytes, s));
   }
   QTX_TRY(copy_block(bs[N - 1], bs[N - 1], batch, x.diag[N - 1], g[N - 1], s));
 
@@ -175,8 +177,8 @@ struct Fp64 {
                    int acc, cudaStream_t s) {
     return ztrace_prod(n, b, X, Y, coef, r, rs, ro, acc, s);
   }
-  static int inv(int n, int64_t b, MatRef X, int* info, MatRef, cudaStream_t s) {
-    return zinv(n, b, X, X, info, nullptr, s);
+  static int inv(int n, int64_t b, MatRef X, int* info, MatRef, void* scr, size_t scr_bytes, cudaStream_t s) {
+    return zinv_ex(n, b, X, X, info, nullptr, scr, scr_bytes, s);
   }
 };
 
@@ -249,10 +251,11 @@ struct Mixed {
     return ctrace_prod(n, b, X, Y, coef, r, rs, ro, acc, s);
   }
   // The Schur complement is inverted in FP64: upcast, Gauss-Jordan, round back.
-  static int inv(int n, int64_t b, MatRef X, int* info, MatRef tmp, cudaStream_t s) {
+  static int inv(int n, int64_t b, MatRef X, int* info, MatRef tmp, void* scr, size_t scr_bytes,
+                 cudaStream_t s) {
     MatRef t = shaped(tmp, n);
     QTX_TRY(convert_c64_to_c128(n, n, b, X, t, s));
-    QTX_TRY(zinv(n, b, t, t, info, nullptr, s));
+    QTX_TRY(zinv_ex(n, b, t, t, info, nullptr, scr, scr_bytes, s));
     return convert_c128_to_c64(n, n, b, t, X, s);
   }
 };
@@ -289,6 +292,8 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
   MatRef tmp[NT_];
   for (int k = 0; k < NT_; ++k) tmp[k] = ws.mat(bm, bm, batch, Prec::E);
   MatRef inv_tmp = Prec::kInvTmp ? ws.mat(bm, bm, batch, sizeof(z64)) : MatRef{};
+  const size_t inv_scr_bytes = zinv_scratch_bytes(bm, batch);
+  void* inv_scr = ws.take(inv_scr_bytes);
   if (ws.base == nullptr) return QTX_OK;
   if (ws.overflow) {
     set_error("selected_solve: workspace too small");
@@ -313,7 +318,7 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
   {
     Addend t[2] = {add(a.diag[0], ONE), add(obc(io.obc_r, 0), MONE)};
     QTX_TRY(Prec::combine(bs[0], bs[0], batch, gR[0], t, 2, s));
-    QTX_TRY(Prec::inv(bs[0], batch, gR[0], info, inv_tmp, s));
+    QTX_TRY(Prec::inv(bs[0], batch, gR[0], info, inv_tmp, inv_scr, inv_scr_bytes, s));
     for (int x = 0; x < 2; ++x) {
       MatRef M = shaped(tmp[M_], bs[0]);
       Addend u[2] = {add(sdiag(x, 0), ONE), add(obc(obx[x], 0), ONE)};
@@ -332,7 +337,7 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
                 .plus(a.diag[j], ONE)
                 .plus(obc(io.obc_r, j), MONE)
                 .run(s));
-    QTX_TRY(Prec::inv(bs[j], batch, gR[j], info, inv_tmp, s));
+    QTX_TRY(Prec::inv(bs[j], batch, gR[j], info, inv_tmp, inv_scr, inv_scr_bytes, s));
     for (int x = 0; x < 2; ++x) {
       MatRef Q{};
       if (!supper(x, i).null()) {

@@ -106,6 +106,7 @@ size_t sancho_rubio_ws(int n, int64_t batch) {
   for (int k = 0; k < 10; ++k) ws.mat(n, n, batch);
   ws.take(sizeof(double) * batch);
   ws.take(sizeof(int) * batch);
+  ws.take(zinv_scratch_bytes(n, batch));
   return ws.off + 256;
 }
 
@@ -115,6 +116,8 @@ struct SRState {
   MatRef eps, eps_s, alpha[2], beta[2], inv_e, aI, bI, t1;
   double* delta;
   int* active;
+  void* scr;  // scratch of the multi-CTA inverse
+  size_t scr_bytes;
 };
 
 SRState sr_state(int n, int64_t batch, Workspace& ws) {
@@ -131,6 +134,8 @@ SRState sr_state(int n, int64_t batch, Workspace& ws) {
   st.t1 = ws.mat(n, n, batch);
   st.delta = static_cast<double*>(ws.take(sizeof(double) * batch));
   st.active = static_cast<int*>(ws.take(sizeof(int) * batch));
+  st.scr_bytes = zinv_scratch_bytes(n, batch);
+  st.scr = ws.take(st.scr_bytes);
   return st;
 }
 
@@ -164,7 +169,7 @@ int sr_iterate(int n, int64_t batch, const SRState& st, int max_iterations, doub
   const int* mask = per_energy ? st.active : nullptr;
   while (it < max_iterations && !done) {
     const int nx = cur ^ 1;
-    QTX_TRY(zinv(n, batch, st.eps, st.inv_e, info, mask, s));
+    QTX_TRY(zinv_ex(n, batch, st.eps, st.inv_e, info, mask, st.scr, st.scr_bytes, s));
     QTX_TRY(G(n, n, n, batch, st.alpha[cur], st.inv_e, st.aI).mask(mask).run(s));
     QTX_TRY(G(n, n, n, batch, st.beta[cur], st.inv_e, st.bI).mask(mask).run(s));
     // t1 = alpha inv beta;  eps_s <- eps_s - t1.
@@ -281,7 +286,7 @@ int sr_iterate_async(int n, int64_t batch, const SRState& st, int max_iterations
   const int* mask = st.active;
   for (int it = 0; it < max_iterations; ++it) {
     const int nx = cur ^ 1;
-    QTX_TRY(zinv(n, batch, st.eps, st.inv_e, info, mask, s));
+    QTX_TRY(zinv_ex(n, batch, st.eps, st.inv_e, info, mask, st.scr, st.scr_bytes, s));
     QTX_TRY(G(n, n, n, batch, st.alpha[cur], st.inv_e, st.aI).mask(mask).run(s));
     QTX_TRY(G(n, n, n, batch, st.beta[cur], st.inv_e, st.bI).mask(mask).run(s));
     QTX_TRY(G(n, n, n, batch, st.aI, st.beta[cur], st.t1)
@@ -331,8 +336,8 @@ int sancho_rubio_multi_async_run(int n, int nsys, const int64_t* batches, const 
   QTX_TRY(sr_iterate_async(n, total, st, max_iterations, tol, per_energy, d_iters, d_converged, info, s));
   off = 0;
   for (int k = 0; k < nsys; ++k) {
-    QTX_TRY(zinv(n, batches[k], offset(st.eps_s, off), from_abi(x[k]), info ? info + off : nullptr,
-                 nullptr, s));
+    QTX_TRY(zinv_ex(n, batches[k], offset(st.eps_s, off), from_abi(x[k]), info ? info + off : nullptr,
+                    nullptr, st.scr, st.scr_bytes, s));
     off += batches[k];
   }
   return QTX_OK;
@@ -351,7 +356,7 @@ int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, M
   if (delta_out)
     QTX_CHECK_CUDA(cudaMemcpyAsync(delta_out, st.delta, sizeof(double) * batch,
                                    cudaMemcpyDeviceToDevice, s));
-  QTX_TRY(zinv(n, batch, st.eps_s, x, info, nullptr, s));
+  QTX_TRY(zinv_ex(n, batch, st.eps_s, x, info, nullptr, st.scr, st.scr_bytes, s));
   return QTX_OK;
 }
 
@@ -374,8 +379,8 @@ int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_ma
   QTX_TRY(sr_iterate(n, total, st, max_iterations, tol, per_energy, iterations, converged, info, s));
   off = 0;
   for (int k = 0; k < nsys; ++k) {
-    QTX_TRY(zinv(n, batches[k], offset(st.eps_s, off), from_abi(x[k]),
-                 info ? info + off : nullptr, nullptr, s));
+    QTX_TRY(zinv_ex(n, batches[k], offset(st.eps_s, off), from_abi(x[k]),
+                    info ? info + off : nullptr, nullptr, st.scr, st.scr_bytes, s));
     off += batches[k];
   }
   return QTX_OK;
@@ -384,19 +389,22 @@ int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_ma
 size_t obc_refine_ws(int n, int64_t batch) {
   Workspace ws;
   for (int k = 0; k < 2; ++k) ws.mat(n, n, batch);
+  ws.take(zinv_scratch_bytes(n, batch));
   return ws.off + 256;
 }
 
 int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, MatRef x, MatRef xref,
                    double* rel, double* abs_res, int* info, Workspace& ws, cudaStream_t s) {
   MatRef T = ws.mat(n, n, batch), S = ws.mat(n, n, batch);
+  const size_t scr_bytes = zinv_scratch_bytes(n, batch);
+  void* scr = ws.take(scr_bytes);
   if (ws.overflow) {
     set_error("obc_refine: workspace too small");
     return QTX_ERR_WORKSPACE;
   }
   QTX_TRY(G(n, n, n, batch, aji, x, T).run(s));
   QTX_TRY(G(n, n, n, batch, T, aij, S, MONE).plus(aii, ONE).run(s));
-  QTX_TRY(zinv(n, batch, S, S, info, nullptr, s));
+  QTX_TRY(zinv_ex(n, batch, S, S, info, nullptr, scr, scr_bytes, s));
   QTX_TRY(znorm_diff(n, batch, S, x, abs_res, nullptr, rel, s));
   Addend t{S, ONE, 0};
   QTX_TRY(zcombine(n, n, batch, xref, &t, 1, nullptr, s));
