@@ -54,6 +54,17 @@ def parse():
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS peak measurements")
     p.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
                    help="fp64 is the headline value; mixed is reported beside it")
+    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4"], default="cfg1",
+                   help="cfg1 (default): the headline line. cfg2: 64 blocks of 512x512, mixed vs FP64. "
+                        "cfg3: eight uneven devices on one GPU. cfg4: the serving loop.")
+    p.add_argument("--cfg3-energies", type=int, default=32, help="energies per device of the uneven batch")
+    p.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the resident solvers")
+    p.add_argument("--cfg4-catalogue", choices=["small", "cfg3"], default="small",
+                   help="serving catalogue: 8 devices with (N, b) drawn as in cfg3 with b in {128, 256} "
+                        "(small) or b in {128, ..., 768} (cfg3)")
+    p.add_argument("--cfg4-rate", type=float, default=None,
+                   help="arrivals per second (default: 0.7 of the measured capacity)")
+    p.add_argument("--cfg4-duration", type=float, default=60.0)
     return p.parse_args()
 
 
@@ -481,11 +492,224 @@ def _ncu_traffic():
     return None
 
 
+def _timed_batches(torch, solver, energies, fl, fr, B, steps, warmup):
+    """Device time of `steps` batches of B energies (cycling through the
+    grid) after `warmup` batches; returns (seconds, clocks)."""
+    nb = max(1, energies.size // B)
+
+    def step(k):
+        i = (k % nb) * B
+        solver.solve(energies[i:i + B], fl[i:i + B], fr[i:i + B])
+
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize()
+    gpu = str(getattr(torch.cuda.get_device_properties(solver.device), "uuid", ""))
+    clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for k in range(steps):
+        step(warmup + k)
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) * 1e-3, clocks.stop()
+
+
+def run_cfg2(args, local):
+    """64 blocks of 512x512 (complex64 storage on the mixed path), 2048
+    energies: mixed energy-points/s beside FP64 on the same grid, and the
+    mixed path's errors in G^R, T and density against FP64."""
+    import torch
+
+    from quatrex_b200 import EnergyPointSolver, synthetic
+    from quatrex_b200.negf import flops_per_energy
+    from quatrex_b200.uneven import jobs_from_devices, plan_batches
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    ne = args.energies if args.energies != 1024 else 2048
+    dev = synthetic.cfg2(ne)
+    job = jobs_from_devices([dev])[0]
+    fl, fr = dev.fermi_left(), dev.fermi_right()
+    out = {}
+    for prec in ("mixed", "fp64"):
+        B = plan_batches([job], args.budget_gb * 1e9, prec)[0]
+        s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True, device=device,
+                              precision=prec, device_loop=True, store_blocks=False)
+        sec, clk = _timed_batches(torch, s, dev.energies, fl, fr, B, args.steps, min(args.warmup, 1))
+        it = s.sr_status(B)[0]
+        out[prec] = {"value": args.steps * B / sec, "batch": B, "seconds": sec, "clocks": clk, "sr_iterations": it}
+        del s
+        torch.cuda.empty_cache()
+    # Error probe: 4 energies with all blocks kept, both precisions.
+    idx = np.linspace(0, ne - 1, 4).astype(int)
+    probe = {}
+    for prec in ("fp64", "mixed"):
+        s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True, device=device,
+                              precision=prec)
+        r = s.solve(dev.energies[idx], fl[idx], fr[idx])
+        probe[prec] = (r.transmission.cpu().numpy().copy(), r.density.cpu().numpy().copy(),
+                       r.blocks["xr_diag"].to(torch.complex128).cpu().numpy())
+        del s, r
+        torch.cuda.empty_cache()
+    f, m = probe["fp64"], probe["mixed"]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    fl_e = flops_per_energy(64, 512, (out["mixed"]["sr_iterations"],) * 2)["total"]
+    line = {
+        "metric": "RGF energy-points/s at 512x512 blocks (mixed)", "value": out["mixed"]["value"],
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": min(args.warmup, 1),
+        "higher_is_better": True, "dtype": "c64 storage, split-TF32 products; FP64 inverses and OBC",
+        "data": "synthetic",
+        "config": {"workload": f"64 blocks of 512x512, {ne} energies in [-3,3], observables only",
+                   "batch_mixed": out["mixed"]["batch"], "batch_fp64": out["fp64"]["batch"],
+                   "budget_gb": args.budget_gb},
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "speedup_vs_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+        "as_written_tflops": {k: v["value"] * fl_e / 1e12 for k, v in out.items()},
+        "error_vs_fp64": {"transmission_max_rel": float(np.max(np.abs(m[0] - f[0]) / np.abs(f[0]))),
+                          "density_rel": rel(m[1], f[1]), "g_retarded_diag_rel": rel(m[2], f[2]),
+                          "probe": f"energies {idx.tolist()}"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_cfg3(args, local):
+    """Eight devices with (N, b) drawn by synthetic.uneven_devices, solved
+    together on one GPU: one captured graph per device, replays on one
+    stream per device, batch sizes planned under the HBM budget."""
+    import torch
+
+    from quatrex_b200 import synthetic
+    from quatrex_b200.uneven import UnevenBatchRunner, jobs_from_devices
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    ne = args.cfg3_energies
+    shapes = synthetic.uneven_devices()
+    devs = [synthetic.make_device(N, b, np.linspace(-2.0, 2.0, ne), seed=0, name=f"dev{k}")
+            for k, (N, b) in enumerate(shapes)]
+    jobs = jobs_from_devices(devs)
+    work = sum(j.flops(19.0) for j in jobs)
+    res, obs = {}, {}
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    for prec in precs:
+        runner = UnevenBatchRunner(jobs, precision=prec, budget_bytes=args.budget_gb * 1e9, device=device)
+        runner.prepare()  # captures every device's graph (one eager pass each)
+        gpu = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
+        clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
+        clocks.start()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        runner.enqueue()
+        t1.record()
+        torch.cuda.synchronize()
+        sec = t0.elapsed_time(t1) * 1e-3
+        res[prec] = {"value": len(jobs) * ne / sec, "seconds": sec, "as_written_tflops": work / sec / 1e12,
+                     "devices": runner.summary(), "sr_converged": all(runner.sr_converged().values()),
+                     "clocks": clocks.stop()}
+        obs[prec] = {k: v["transmission"].cpu().numpy().copy() for k, v in runner.results().items()}
+        del runner
+        torch.cuda.empty_cache()
+    line = {
+        "metric": "RGF energy-points/s, uneven batch of 8 devices", "value": res[precs[0]]["value"],
+        "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True,
+        "dtype": precs[0], "data": "synthetic",
+        "config": {"workload": f"8 devices (N, b) = {shapes}, {ne} energies each in [-2,2], observables only",
+                   "budget_gb": args.budget_gb, "step": "every energy of every device, one pass",
+                   "warmup": "the capture pass of each device's graph"},
+        "results": res,
+    }
+    if len(precs) == 2:
+        line["speedup_mixed_vs_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+        line["mixed_transmission_max_rel_vs_fp64"] = max(
+            float(np.max(np.abs(obs["mixed"][k] - obs["fp64"][k]) / np.abs(obs["fp64"][k]))) for k in obs["fp64"])
+    print(json.dumps(line), flush=True)
+
+
+def run_cfg4(args, local):
+    """The serving loop: Poisson arrivals of requests (one catalogue device,
+    64-512 of its 512 grid energies each), continuous batching per device
+    lane, HBM-budget admission, resident OBC warm starts. Reports p50/p99
+    request latency (host clock, arrival to completion) and served
+    energy-points/s, FP64 and mixed on the same request trace."""
+    import torch
+
+    from quatrex_b200 import synthetic
+    from quatrex_b200.negf import flops_per_energy
+    from quatrex_b200.serving import EnergyServer, poisson_requests
+    from quatrex_b200.uneven import jobs_from_devices
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    bsz = (128, 256) if args.cfg4_catalogue == "small" else (128, 256, 384, 512, 768)
+    shapes = synthetic.uneven_devices(block_sizes=bsz)
+    grid = 512
+    devs = [synthetic.make_device(N, b, np.linspace(-2.0, 2.0, grid), seed=0, name=f"dev{k}")
+            for k, (N, b) in enumerate(shapes)]
+    cat = jobs_from_devices(devs)
+    mean_n = (64 + 512) / 2
+    req_flops = np.mean([flops_per_energy(N, b, (19, 19))["total"] * mean_n for N, b in shapes])
+    spec_shapes = synthetic.uneven_devices()
+    spec_req_flops = np.mean([flops_per_energy(N, b, (19, 19))["total"] * mean_n for N, b in spec_shapes])
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    out, rate = {}, args.cfg4_rate
+    for prec in precs:
+        srv = EnergyServer(cat, precision=prec, budget_bytes=args.budget_gb * 1e9, warm_start=True,
+                           device=device)
+        if rate is None:  # 0.7 of the capacity measured on one cold replay per lane, lanes run back to back
+            per_energy = []
+            for ln in srv.lanes:
+                t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(ln.stream):
+                    t0.record()
+                    ln.graphs[False].replay()
+                    t1.record()
+                torch.cuda.synchronize()
+                per_energy.append(t0.elapsed_time(t1) * 1e-3 / ln.B)
+            rate = 0.7 / (mean_n * float(np.mean(per_energy)))
+        reqs = poisson_requests(rate, args.cfg4_duration, [grid] * len(cat), (64, 512), seed=0)
+        gpu = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
+        clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
+        clocks.start()
+        stats = srv.run(reqs)
+        stats["clocks"] = clocks.stop()
+        stats["as_written_tflops"] = stats["energies"] * req_flops / mean_n / stats["wall_s"] / 1e12
+        out[prec] = stats
+        del srv
+        torch.cuda.empty_cache()
+    main = out[precs[0]]
+    line = {
+        "metric": "serving: energy-points/s and p50/p99 request latency", "value": main["energies_per_s"],
+        "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "dtype": precs[0],
+        "data": "synthetic",
+        "config": {"workload": f"Poisson arrivals at {rate:.3g} req/s for {args.cfg4_duration:g} s, seed 0; "
+                               f"catalogue of 8 devices (N, b) = {shapes}, 512-point grids on [-2,2]; "
+                               "64-512 grid energies per request",
+                   "rate_rule": "given" if args.cfg4_rate else "0.7 of the capacity measured per lane",
+                   "budget_gb": args.budget_gb, "warm_starts": True,
+                   "latency_clock": "host wall clock, arrival to completion"},
+        "p50_s": main["latency"].get("p50_s"), "p99_s": main["latency"].get("p99_s"),
+        "results": out,
+        "offered_load_note": {
+            "spec_rate_req_s": 200, "spec_mean_request_tflop": spec_req_flops / 1e12,
+            "spec_demand_pflops": 200 * spec_req_flops / 1e15,
+            "this_catalogue_mean_request_tflop": req_flops / 1e12},
+    }
+    if len(precs) == 2:
+        line["speedup_mixed_vs_fp64"] = out["mixed"]["energies_per_s"] / out["fp64"]["energies_per_s"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload != "cfg1":
+        if rank == 0:
+            {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4}[args.workload](args, local)
         return
     run_ours(args, world, rank, local)
 

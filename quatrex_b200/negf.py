@@ -127,9 +127,45 @@ class EnergyPointSolver:
         # Workspaces belong to this solver: captured graphs hold their
         # addresses, and solvers on concurrent streams must not share them.
         self._ws = WorkspacePool()
+        self._grid = None  # (energies, f_left, f_right) on the device, see bind_grid
+        self._cache = None  # resident surface Green's functions, see enable_obc_cache
         self.lib = _native.load()
 
     # ------------------------------------------------------------------
+    def bind_grid(self, energies, f_left, f_right) -> None:
+        """Keeps an energy grid (with lead occupations) on the device. A batch
+        is then named by grid indices (:meth:`set_indices`) and the captured
+        pipeline gathers its energies itself, so one replay needs only the
+        index vector as input."""
+        dev = self.device
+        as_dev = lambda x: torch.as_tensor(np.asarray(x, dtype=np.float64)).reshape(-1).to(dev)  # noqa: E731
+        self._grid = (as_dev(energies), as_dev(f_left), as_dev(f_right))
+        self._bufs.clear()
+        self._graphs.clear()
+
+    def enable_obc_cache(self) -> None:
+        """Resident warm starts: the refined surface Green's functions of
+        every grid energy solved so far stay on the device (two b x b blocks
+        per grid point). A warm run reads them instead of running
+        Sancho-Rubio and applies the OBCSystem fixed-point step
+        (``boundary_system.py:303-373``) to them."""
+        if self._grid is None:
+            raise RuntimeError("enable_obc_cache() needs bind_grid() first")
+        G = int(self._grid[0].numel())
+        z = lambda: torch.zeros((G, self.b, self.b), dtype=_C128, device=self.device)  # noqa: E731
+        self._cache = (z(), z())
+        self._graphs.clear()
+
+    def cache_bytes(self) -> int:
+        return 0 if self._grid is None else 2 * int(self._grid[0].numel()) * self.b * self.b * 16
+
+    def set_indices(self, idx) -> int:
+        """Grid indices of the next batch (see bind_grid)."""
+        t = torch.as_tensor(np.asarray(idx, dtype=np.int64)).reshape(-1)
+        B = int(t.numel())
+        self._buffers(B)["idx"].copy_(t)
+        return B
+
     def resident_bytes(self, B: int) -> int:
         """Device bytes this solver holds for batch size B (buffers and
         workspaces), without allocating anything."""
@@ -161,6 +197,8 @@ class EnergyPointSolver:
             res_abs=[torch.empty(B, dtype=torch.float64, device=dev) for _ in range(2)],
             sr_it=torch.zeros(1, dtype=torch.int32, device=dev), sr_conv=torch.zeros(1, dtype=torch.int32, device=dev),
         )
+        if self._grid is not None:
+            buf["idx"] = torch.zeros(B, dtype=torch.int64, device=dev)
         if self.precision == "mixed":
             buf["a_diag64"] = o(N, B, b, b)
             buf["sig64"] = [o(B, b, b) for _ in range(6)]
@@ -193,6 +231,8 @@ class EnergyPointSolver:
     def set_inputs(self, energies, f_left, f_right) -> int:
         """Copies one batch's energies and occupations into the solver's
         device input buffers (the only per-batch host-to-device traffic)."""
+        if self._grid is not None:
+            raise RuntimeError("this solver is bound to an energy grid: name batches with set_indices()")
         dev = self.device
         E = torch.as_tensor(np.asarray(energies, dtype=np.float64)).reshape(-1)
         B = int(E.numel())
@@ -212,26 +252,26 @@ class EnergyPointSolver:
         buf["fr"].copy_(f_right.reshape(-1), non_blocking=True)
         return B
 
-    def capture(self, B: int) -> "torch.cuda.CUDAGraph":
+    def capture(self, B: int, warm: bool = False) -> "torch.cuda.CUDAGraph":
         """Captures the whole energy-point pipeline for batch size B in one
         CUDA graph (Sancho-Rubio runs its device-side convergence loop). The
         inputs are read from the solver's device buffers, so a replay after
         set_inputs() solves a new batch. The first capture runs the pipeline
         once eagerly to allocate every buffer outside the capture."""
-        g = self._graphs.get(B)
+        g = self._graphs.get((B, warm))
         if g is not None:
             return g
         self._buffers(B)
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
-            self._run(B, device_loop=True)
+            self._run(B, device_loop=True, warm=warm)
         torch.cuda.current_stream(self.device).wait_stream(side)
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=side):
-            self._run(B, device_loop=True)
-        self._graphs[B] = g
+            self._run(B, device_loop=True, warm=warm)
+        self._graphs[(B, warm)] = g
         return g
 
     def solve_graph(self, energies, f_left, f_right) -> PointResult:
@@ -257,7 +297,7 @@ class EnergyPointSolver:
         its = (self._host_sr[0],) * 2 if not self._last_device_loop else ("device", "device")
         return PointResult(buf["T"], buf["density"], buf["current"], sig[0], sig[3], its, blocks)
 
-    def _run(self, B: int, device_loop: bool) -> PointResult:
+    def _run(self, B: int, device_loop: bool, warm: bool = False) -> PointResult:
         """The kernel sequence of one batch; no host transfers, and no host
         synchronisation when device_loop is set (graph-capturable)."""
         lib, dev = self.lib, self.device
@@ -267,6 +307,11 @@ class EnergyPointSolver:
         keep: list = []
         self._last_device_loop = device_loop
         fl, fr = buf["fl"], buf["fr"]
+        if self._grid is not None:  # the batch is named by grid indices
+            idx = buf["idx"]
+            torch.index_select(self._grid[0], 0, idx, out=buf["E"])
+            torch.index_select(self._grid[1], 0, idx, out=fl)
+            torch.index_select(self._grid[2], 0, idx, out=fr)
         _native.check(lib.qtx_assemble_energies(B, buf["E"].data_ptr(), float(self.eta), buf["zE"].data_ptr(),
                                                 stream))
 
@@ -282,7 +327,13 @@ class EnergyPointSolver:
         sig = buf["sig"]
         sides = ((a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
                  (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))
-        self._sr_both(sides, B, stream, device_loop, buf)
+        if warm:
+            if self._cache is None:
+                raise RuntimeError("a warm run needs enable_obc_cache()")
+            torch.index_select(self._cache[0], 0, buf["idx"], out=buf["gl"])
+            torch.index_select(self._cache[1], 0, buf["idx"], out=buf["gr"])
+        else:
+            self._sr_both(sides, B, stream, device_loop, buf)
         for k, (aii, aij, aji, g, f, s3) in enumerate(sides):
             ws = self._ws.get(lib.qtx_obc_workspace(b, B), dev, "obc")
             _native.check(lib.qtx_obc_refine(b, B, mat(aii), aij, aji, mat(g), mat(g),
@@ -291,6 +342,9 @@ class EnergyPointSolver:
             _native.check(lib.qtx_contact_self_energy(b, B, aij, aji, mat(g), f.data_ptr(), mat(s3[0]),
                                                       mat(s3[1]), mat(s3[2]), ws.data_ptr(), ws.numel(),
                                                       stream))
+        if self._cache is not None:
+            self._cache[0].index_copy_(0, buf["idx"], buf["gl"])
+            self._cache[1].index_copy_(0, buf["idx"], buf["gr"])
         self.last_residuals = (torch.maximum(buf["res_rel"][0], buf["res_rel"][1]) if not device_loop
                                else buf["res_rel"][0], buf["res_abs"][0])
 
