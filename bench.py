@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS peak measurements")
     p.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
                    help="fp64 is the headline value; mixed is reported beside it")
-    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4"], default="cfg1",
+    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels"], default="cfg1",
                    help="cfg1 (default): the headline line. cfg2: 64 blocks of 512x512, mixed vs FP64. "
                         "cfg3: eight uneven devices on one GPU. cfg4: the serving loop.")
     p.add_argument("--cfg3-energies", type=int, default=32, help="energies per device of the uneven batch")
@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--cfg4-rate", type=float, default=None,
                    help="arrivals per second (default: 0.7 of the measured capacity)")
     p.add_argument("--cfg4-duration", type=float, default=60.0)
+    p.add_argument("--inverse-path", choices=["auto", "single", "wide"], default="auto",
+                   help="inverse kernels: automatic choice, one CTA per matrix, or multi-CTA panels")
     return p.parse_args()
 
 
@@ -466,7 +468,8 @@ def run_ours(args, world, rank, local):
         "dtype": "f64 (complex128)" if main_prec == "fp64" else "c64 storage, split-TF32 products",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "batch": B, "energies": args.energies,
-                   "parallelism": f"energy sharding x{world}", "l2": "inputs exceed L2 (resident batch state "
+                   "parallelism": f"energy sharding x{world}", "inverse_path": args.inverse_path,
+                   "l2": "inputs exceed L2 (resident batch state "
                    f"~{B * 0.45:.0f} GB)", "sr_iterations_mean": [float(x) for x in its]},
         "roofline": roofline,
         "as_written_tflops": value * fl["total"] / 1e12,
@@ -701,15 +704,86 @@ def run_cfg4(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_kernels(args, local):
+    """Kernel-level rooflines at the cfg1 block shape: batched complex GEMMs
+    (ours and cuBLAS through torch on the same shapes) and batched inverses
+    (ours, both paths, and torch.linalg.inv), CUDA-event timed, inputs
+    resident (batch x 3 blocks of 1 MiB each > L2 for batch 148)."""
+    import ctypes
+
+    import torch
+
+    from quatrex_b200 import _native
+    from quatrex_b200._interop import mat
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    lib = _native.load()
+    n, B = 256, args.batch
+    stream = lambda: ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # noqa: E731
+    g = torch.Generator(device=device).manual_seed(0)
+
+    def rnd(dt):
+        return torch.randn((B, n, n), dtype=dt, device=device, generator=g)
+
+    def timeit(fn, reps=max(args.steps, 3)):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps * 1e-3
+
+    flops = 8.0 * n ** 3 * B
+    out = {}
+    a, b, c = rnd(torch.complex128), rnd(torch.complex128), torch.empty((B, n, n), dtype=torch.complex128,
+                                                                         device=device)
+    z = _native.NULL_MAT
+    out["zgemm_ours"] = flops / timeit(lambda: _native.check(lib.qtx_zgemm_batched(
+        n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 0, 0.0, 0.0, z, 0, mat(c), stream()))) / 1e12
+    out["zgemm_cublas_bmm"] = flops / timeit(lambda: torch.bmm(a, b, out=c)) / 1e12
+    a32, b32, c32 = a.to(torch.complex64), b.to(torch.complex64), c.to(torch.complex64)
+    out["cgemm_ours_split_tf32"] = flops / timeit(lambda: _native.check(lib.qtx_cgemm_batched(
+        n, n, n, B, 1.0, 0.0, mat(a32), 0, mat(b32), 0, 0.0, 0.0, z, 0, mat(c32), None, stream()))) / 1e12
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    out["cgemm_cublas_bmm_tf32_allowed"] = flops / timeit(lambda: torch.bmm(a32, b32, out=c32)) / 1e12
+    torch.backends.cuda.matmul.allow_tf32 = old
+    del a32, b32, c32
+    eye = torch.eye(n, dtype=torch.complex128, device=device)
+    w = (a + n * eye).contiguous()  # well conditioned
+    info = torch.zeros(B, dtype=torch.int32, device=device)
+    ws = torch.empty(lib.qtx_zinv_workspace(n, B), dtype=torch.uint8, device=device)
+    for name, mode in (("zinv_ours_one_cta_per_matrix", 1), ("zinv_ours_multi_cta", 2)):
+        _native.check(lib.qtx_set_inverse_path(mode))
+        out[name] = flops / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
+            n, B, mat(w), mat(c), info.data_ptr(), ws.data_ptr(), ws.numel(), stream()))) / 1e12
+    _native.check(lib.qtx_set_inverse_path(0))
+    out["zinv_torch_linalg_inv"] = flops / timeit(lambda: torch.linalg.inv(w)) / 1e12
+    peak = None if args.no_peak else measured_fp64_peak(torch, device)["peak"]
+    tf32 = None if args.no_peak else measured_tf32_peak(torch, device)
+    line = {"metric": "kernel throughput at 256x256 blocks (complex flops 8n^3)", "unit": "TFLOP/s",
+            "batch": B, "results": out, "fp64_peak_measured": peak, "tf32_peak_measured": tf32,
+            "note": "inverse flops counted as 8n^3 like a GEMM; cuBLAS/cuSOLVER legs are library references"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
+    from quatrex_b200 import _native
+
+    _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2}[args.inverse_path]))
     if args.workload != "cfg1":
         if rank == 0:
-            {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4}[args.workload](args, local)
+            {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels}[args.workload](args, local)
         return
     run_ours(args, world, rank, local)
 

@@ -287,11 +287,14 @@ int num_sms() {
   return sms;
 }
 
+// Panel width: as wide as the n x NB panel fits in shared memory.
+int panel_width(int n) { return n <= 416 ? 32 : (n <= 832 ? 16 : 8); }
+
 }  // namespace
 
 size_t zinv_scratch_bytes(int n, int64_t batch) {
   if (n <= 0 || batch <= 0) return 0;
-  const int nb = n <= 832 ? 16 : 8;
+  const int nb = panel_width(n);
   return (size_t)batch * ((size_t)nb * n * sizeof(z64) + 2 * (size_t)n * sizeof(int)) + 1024;
 }
 
@@ -315,13 +318,14 @@ int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* acti
     set_error("zinv: null matrix");
     return QTX_ERR_ARG;
   }
-  const int nb = n <= 832 ? 16 : 8;
+  const int nb = panel_width(n);
   char* p = static_cast<char*>(scratch);
   p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 255) & ~uintptr_t(255));
   Scratch sc;
   sc.Y = reinterpret_cast<z64*>(p);
   sc.piv = reinterpret_cast<int*>(sc.Y + (size_t)batch * nb * n);
   sc.colsrc = sc.piv + (size_t)batch * n;
+  if (nb == 32) return run_wide<32>(n, batch, A, X, info, active, sc, s);
   if (nb == 16) return run_wide<16>(n, batch, A, X, info, active, sc, s);
   return run_wide<8>(n, batch, A, X, info, active, sc, s);
 }
