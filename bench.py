@@ -746,6 +746,14 @@ def run_kernels(args, local):
     out["zgemm_ours"] = flops / timeit(lambda: _native.check(lib.qtx_zgemm_batched(
         n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 0, 0.0, 0.0, z, 0, mat(c), stream()))) / 1e12
     out["zgemm_cublas_bmm"] = flops / timeit(lambda: torch.bmm(a, b, out=c)) / 1e12
+    d2 = rnd(torch.complex128)
+    out["zgemm_ours_plus_ct_addend"] = flops / timeit(lambda: _native.check(lib.qtx_zgemm_batched(
+        n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 0, 1.0, 0.0, mat(d2), 1, mat(c), stream()))) / 1e12
+    out["zgemm_ours_plus_addend"] = flops / timeit(lambda: _native.check(lib.qtx_zgemm_batched(
+        n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 0, 1.0, 0.0, mat(d2), 0, mat(c), stream()))) / 1e12
+    out["zgemm_ours_b_conj_trans"] = flops / timeit(lambda: _native.check(lib.qtx_zgemm_batched(
+        n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 1, 0.0, 0.0, z, 0, mat(c), stream()))) / 1e12
+    del d2
     a32, b32, c32 = a.to(torch.complex64), b.to(torch.complex64), c.to(torch.complex64)
     out["cgemm_ours_split_tf32"] = flops / timeit(lambda: _native.check(lib.qtx_cgemm_batched(
         n, n, n, B, 1.0, 0.0, mat(a32), 0, mat(b32), 0, 0.0, 0.0, z, 0, mat(c32), None, stream()))) / 1e12

@@ -19,7 +19,10 @@
 // fuses up to four scaled (optionally conjugate-transposed) addends, a
 // conjugate-transposed second store and a second output with its own
 // addends, so chains like  S = A_jj - Sigma - P A_ij  or
-// X_ij = -X_ii A X_jj  with  X_ji = -X_ij^H  are one launch.
+// X_ij = -X_ii A X_jj  with  X_ji = -X_ij^H  are one launch. It runs through
+// a padded shared-memory tile: transposed operands are read and written with
+// lanes along rows, the others with lanes along columns (coalesced both ways,
+// many independent loads in flight).
 #include "common.cuh"
 
 namespace qtx {
@@ -42,6 +45,7 @@ constexpr int A_MK_SIZE = BM * S_MK;
 constexpr int A_KM_SIZE = BK * S_KM;
 constexpr int B_NK_SIZE = BN * S_MK;
 constexpr int B_KN_SIZE = BK * (BN + 2);
+constexpr int TS = BN + 1;  // epilogue tile row stride (complex): 1 mod 8 in 16-byte units
 
 __device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, double b0) {
   asm volatile(
@@ -220,37 +224,89 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
     cp_async_wait<0>();
     __syncthreads();
 
-    // Epilogue.
+    // Epilogue through a padded shared-memory tile (it reuses the stage
+    // buffers) so that global reads and writes are coalesced in either
+    // orientation. Phase A (fragment layout, lanes mostly along rows):
+    // alpha * acc + the conjugate-transposed addends -> tile.
+    z64* tile = smem;
 #pragma unroll
     for (int i = 0; i < MT; ++i)
 #pragma unroll
       for (int j = 0; j < NT; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const int r = m0 + wm0 + i * 16 + g + ((q >> 1) << 3);
-          const int c = n0 + wn0 + j * 8 + 2 * tq + (q & 1);
-          if (r >= M || c >= N) continue;
-          z64 v = zmul(d.alpha, make_double2(acc_re[i][j][q], acc_im[i][j][q]));
-          for (int t = 0; t < d.nadd; ++t) {
-            const Addend& ad = d.add[t];
-            const z64* p = at<const z64>(ad.m, b);
-            const z64 x = ad.conj_trans ? zconj(p[(int64_t)c * ad.m.ld + r]) : p[(int64_t)r * ad.m.ld + c];
-            v = zfma(ad.coef, x, v);
-          }
-          if (!d.C3.null()) {
-            z64 v3 = zmul(d.scale3, v);
-            for (int t = d.nadd; t < d.nadd + d.nadd3; ++t) {
-              const Addend& ad = d.add[t];
-              const z64* p = at<const z64>(ad.m, b);
-              const z64 x =
-                  ad.conj_trans ? zconj(p[(int64_t)c * ad.m.ld + r]) : p[(int64_t)r * ad.m.ld + c];
-              v3 = zfma(ad.coef, x, v3);
-            }
-            at<z64>(d.C3, b)[(int64_t)r * d.C3.ld + c] = v3;
-          }
-          if (!d.C2.null()) at<z64>(d.C2, b)[(int64_t)c * d.C2.ld + r] = zmul(d.coef2, zconj(v));
-          if (!d.C.null()) at<z64>(d.C, b)[(int64_t)r * d.C.ld + c] = v;
+          const int rl = wm0 + i * 16 + g + ((q >> 1) << 3);
+          const int cl = wn0 + j * 8 + 2 * tq + (q & 1);
+          tile[rl * TS + cl] = zmul(d.alpha, make_double2(acc_re[i][j][q], acc_im[i][j][q]));
         }
+    for (int t = 0; t < d.nadd; ++t) {
+      const Addend& ad = d.add[t];
+      if (!ad.conj_trans) continue;
+      const z64* p = at<const z64>(ad.m, b);
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int rl = wm0 + i * 16 + g + ((q >> 1) << 3);
+            const int cl = wn0 + j * 8 + 2 * tq + (q & 1);
+            const int r = m0 + rl, c = n0 + cl;
+            if (r < M && c < N)
+              tile[rl * TS + cl] = zfma(ad.coef, zconj(p[(int64_t)c * ad.m.ld + r]), tile[rl * TS + cl]);
+          }
+    }
+    __syncthreads();
+    // Phase B (lanes along columns): the other addends, C3 and C.
+    for (int t = 0; t < d.nadd; ++t) {
+      const Addend& ad = d.add[t];
+      if (ad.conj_trans) continue;
+      const z64* p = at<const z64>(ad.m, b);
+#pragma unroll 8
+      for (int e = tid; e < BM * BN; e += THREADS) {
+        const int rl = e / BN, cl = e % BN;
+        const int r = m0 + rl, c = n0 + cl;
+        if (r < M && c < N) tile[rl * TS + cl] = zfma(ad.coef, p[(int64_t)r * ad.m.ld + c], tile[rl * TS + cl]);
+      }
+    }
+    if (!d.C3.null()) {
+#pragma unroll 4
+      for (int e = tid; e < BM * BN; e += THREADS) {
+        const int rl = e / BN, cl = e % BN;
+        const int r = m0 + rl, c = n0 + cl;
+        if (r >= M || c >= N) continue;
+        z64 v3 = zmul(d.scale3, tile[rl * TS + cl]);
+        for (int t = d.nadd; t < d.nadd + d.nadd3; ++t) {
+          const Addend& ad = d.add[t];
+          const z64* p = at<const z64>(ad.m, b);
+          const z64 x = ad.conj_trans ? zconj(p[(int64_t)c * ad.m.ld + r]) : p[(int64_t)r * ad.m.ld + c];
+          v3 = zfma(ad.coef, x, v3);
+        }
+        at<z64>(d.C3, b)[(int64_t)r * d.C3.ld + c] = v3;
+      }
+    }
+    if (!d.C.null()) {
+      z64* out = at<z64>(d.C, b);
+#pragma unroll 8
+      for (int e = tid; e < BM * BN; e += THREADS) {
+        const int rl = e / BN, cl = e % BN;
+        const int r = m0 + rl, c = n0 + cl;
+        if (r < M && c < N) out[(int64_t)r * d.C.ld + c] = tile[rl * TS + cl];
+      }
+    }
+    // Phase C (lanes along rows): the conjugate-transposed second store,
+    // after every thread's phase-B updates of the tile.
+    if (!d.C2.null()) {
+      __syncthreads();
+      z64* out2 = at<z64>(d.C2, b);
+#pragma unroll 8
+      for (int e = tid; e < BM * BN; e += THREADS) {
+        const int rl = e % BM, cl = e / BM;
+        const int r = m0 + rl, c = n0 + cl;
+        if (r < M && c < N) out2[(int64_t)c * d.C2.ld + r] = zmul(d.coef2, zconj(tile[rl * TS + cl]));
+      }
+    }
+    __syncthreads();  // the tile aliases the stage buffers of the next entry
   }
 }
 
@@ -258,7 +314,9 @@ template <int OPA, int OPB>
 int launch(const GemmDesc& d, cudaStream_t s) {
   constexpr int A_SIZE = (OPA == 0) ? A_MK_SIZE : A_KM_SIZE;
   constexpr int B_SIZE = (OPB == 1) ? B_NK_SIZE : B_KN_SIZE;
-  constexpr size_t smem = STAGES * (A_SIZE + B_SIZE) * sizeof(z64);
+  constexpr size_t stages = STAGES * (A_SIZE + B_SIZE) * sizeof(z64);
+  constexpr size_t tile = (size_t)BM * TS * sizeof(z64);
+  constexpr size_t smem = stages > tile ? stages : tile;
   QTX_CHECK_CUDA(cudaFuncSetAttribute(zgemm_kernel<OPA, OPB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((d.N + BN - 1) / BN, (d.M + BM - 1) / BM,
