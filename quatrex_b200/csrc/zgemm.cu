@@ -243,6 +243,17 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
       const Addend& ad = d.add[t];
       if (!ad.conj_trans) continue;
       const z64* p = at<const z64>(ad.m, b);
+      z64 x[MT][NT][4];  // all loads first: many in flight, no aliasing stalls
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = m0 + wm0 + i * 16 + g + ((q >> 1) << 3);
+            const int c = n0 + wn0 + j * 8 + 2 * tq + (q & 1);
+            x[i][j][q] = (r < M && c < N) ? p[(int64_t)c * ad.m.ld + r] : make_double2(0.0, 0.0);
+          }
 #pragma unroll
       for (int i = 0; i < MT; ++i)
 #pragma unroll
@@ -251,22 +262,28 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
           for (int q = 0; q < 4; ++q) {
             const int rl = wm0 + i * 16 + g + ((q >> 1) << 3);
             const int cl = wn0 + j * 8 + 2 * tq + (q & 1);
-            const int r = m0 + rl, c = n0 + cl;
-            if (r < M && c < N)
-              tile[rl * TS + cl] = zfma(ad.coef, zconj(p[(int64_t)c * ad.m.ld + r]), tile[rl * TS + cl]);
+            tile[rl * TS + cl] = zfma(ad.coef, zconj(x[i][j][q]), tile[rl * TS + cl]);
           }
     }
     __syncthreads();
     // Phase B (lanes along columns): the other addends, C3 and C.
+    constexpr int PER = BM * BN / THREADS;  // elements per thread
     for (int t = 0; t < d.nadd; ++t) {
       const Addend& ad = d.add[t];
       if (ad.conj_trans) continue;
       const z64* p = at<const z64>(ad.m, b);
-#pragma unroll 8
-      for (int e = tid; e < BM * BN; e += THREADS) {
+      z64 x[PER];  // all loads first: many in flight, no aliasing stalls
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int e = tid + k * THREADS;
+        const int r = m0 + e / BN, c = n0 + e % BN;
+        x[k] = (r < M && c < N) ? p[(int64_t)r * ad.m.ld + c] : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int e = tid + k * THREADS;
         const int rl = e / BN, cl = e % BN;
-        const int r = m0 + rl, c = n0 + cl;
-        if (r < M && c < N) tile[rl * TS + cl] = zfma(ad.coef, p[(int64_t)r * ad.m.ld + c], tile[rl * TS + cl]);
+        tile[rl * TS + cl] = zfma(ad.coef, x[k], tile[rl * TS + cl]);
       }
     }
     if (!d.C3.null()) {
