@@ -354,6 +354,334 @@ int launch(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* activ
   return QTX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Second generation (n <= 720): the same Gauss-Jordan with the same pivot
+// rule, reorganised so that the trailing update runs without barriers.
+// Per panel of NB columns:
+//   1. stage the n x NB panel (odd row stride: row-per-thread access is
+//      conflict-free) and factor it (one barrier pair per column, the next
+//      column's pivot candidate found during the elimination);
+//   2. apply the panel's row interchanges to the other columns in global
+//      memory: the <= 2 NB affected rows are read into registers, then
+//      written to their new places;
+//   3. stage the pivot rows Y = X[K, :] (other columns) once;
+//   4. every warp updates its 16-row slices over all column tiles:
+//      X[r, J] = (r in K ? 0 : X[r, J]) + T[r, :] Y[:, J]  (DMMA), with no
+//      barrier, so 16 warps overlap their loads and MMAs;
+//   5. write the panel transform T back into X[:, K].
+constexpr int T2 = 512;
+constexpr int W2 = T2 / 32;
+constexpr int JN = 2;    // n8 tiles per column tile of the trailing update
+constexpr int CW = 128;  // column block of the row-interchange pass
+constexpr int PV = 8;    // its elements per thread: 2 NB rows x CW columns <= T2 x PV for NB <= 16
+
+template <int NB>
+struct Smem2 {
+  static constexpr int PS = NB + 1;
+  // Y row stride: covers whole 16-column tiles, 2 mod 8 in 16-byte units.
+  __host__ __device__ static int ys(int n) { return ((n + 15) / 16) * 16 + 2; }
+  static size_t bytes(int n) {
+    size_t s = (size_t)n * PS * sizeof(z64);          // panel
+    s += (size_t)NB * ys(n) * sizeof(z64);            // pivot rows Y
+    s += (size_t)2 * NB * sizeof(z64);                // scaled pivot row, old row k
+    s += (size_t)2 * W2 * (sizeof(double) + sizeof(int));
+    s += (size_t)2 * (2 * NB) * sizeof(int);          // affected rows and their sources
+    s += (size_t)2 * n * sizeof(int) + 16;            // pivot rows, column sources
+    return s + 64;
+  }
+};
+
+template <int NB>
+__global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatRef A, MatRef X, int* info,
+                                                      const int* active) {
+  using S = Smem2<NB>;
+  static_assert(2 * NB * CW <= T2 * PV, "interchange block must fit the per-thread registers");
+  constexpr int PS = S::PS;
+  const int YS = S::ys(n);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  z64* P = reinterpret_cast<z64*>(smem_raw);
+  z64* Y = P + (size_t)n * PS;
+  z64* prow = Y + (size_t)NB * YS;
+  z64* rowk = prow + NB;
+  double* red_v = reinterpret_cast<double*>(rowk + NB);  // 2 x W2
+  int* red_i = reinterpret_cast<int*>(red_v + 2 * W2);   // 2 x W2
+  int* aff_row = red_i + 2 * W2;                         // 2 NB
+  int* aff_src = aff_row + 2 * NB;                       // 2 NB
+  int* pivrow = aff_src + 2 * NB;                        // n
+  int* colsrc = pivrow + n;                              // n
+  __shared__ int s_na;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    if (active != nullptr && active[b] == 0) continue;
+    const z64* a = at<const z64>(A, b);
+    z64* x = at<z64>(X, b);
+    const int64_t ldx = X.ld;
+    if (a != x) {
+      for (int64_t idx = tid; idx < (int64_t)n * n; idx += T2) {
+        const int r = (int)(idx / n), c = (int)(idx % n);
+        x[(int64_t)r * ldx + c] = a[(int64_t)r * A.ld + c];
+      }
+    }
+    int singular_at = 0;
+    __syncthreads();
+
+    for (int k0 = 0; k0 < n; k0 += NB) {
+      const int nbp = min(NB, n - k0);
+      // 1. Stage and factor the panel.
+      for (int idx = tid; idx < n * NB; idx += T2) {
+        const int r = idx / NB, c = idx % NB;
+        P[r * PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+      double best = -1.0;
+      int besti = k0;
+      for (int r = k0 + tid; r < n; r += T2) {
+        const double v = cabs1(P[r * PS]);
+        if (v > best || (v == best && r < besti)) {
+          best = v;
+          besti = r;
+        }
+      }
+      for (int kk = 0; kk < nbp; ++kk) {
+        const int k = k0 + kk;
+        const int buf = kk & 1;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+          const int oi = __shfl_xor_sync(0xffffffffu, besti, off);
+          if (ov > best || (ov == best && oi < besti)) {
+            best = ov;
+            besti = oi;
+          }
+        }
+        if (lane == 0) {
+          red_v[buf * W2 + warp] = best;
+          red_i[buf * W2 + warp] = besti;
+        }
+        __syncthreads();
+        best = red_v[buf * W2];
+        besti = red_i[buf * W2];
+#pragma unroll
+        for (int w = 1; w < W2; ++w) {
+          const double ov = red_v[buf * W2 + w];
+          const int oi = red_i[buf * W2 + w];
+          if (ov > best || (ov == best && oi < besti)) {
+            best = ov;
+            besti = oi;
+          }
+        }
+        const int p = besti;
+        if (best <= 0.0 && singular_at == 0) singular_at = k + 1;
+        const z64 dpiv = zrecip(P[p * PS + kk]);
+        if (tid < NB) {
+          rowk[tid] = P[k * PS + tid];
+          prow[tid] = (tid == kk) ? dpiv : zmul(P[p * PS + tid], dpiv);
+        }
+        if (tid == 0) pivrow[k] = p;
+        __syncthreads();
+        best = -1.0;
+        besti = k + 1;
+        for (int r = tid; r < n; r += T2) {
+          if (r == k) {
+#pragma unroll
+            for (int c = 0; c < NB; ++c) P[r * PS + c] = prow[c];
+            continue;
+          }
+          const z64* src = (r == p) ? rowk : P + r * PS;
+          const z64 f = src[kk];
+#pragma unroll
+          for (int c = 0; c < NB; ++c) {
+            if (c == kk) continue;
+            const z64 v = src[c];
+            const z64 q = prow[c];
+            P[r * PS + c] = make_double2(v.x - (f.x * q.x - f.y * q.y), v.y - (f.x * q.y + f.y * q.x));
+          }
+          const z64 m = zmul(f, dpiv);
+          P[r * PS + kk] = make_double2(-m.x, -m.y);
+          if (kk + 1 < nbp && r > k) {
+            const double v = cabs1(P[r * PS + kk + 1]);
+            if (v > best || (v == best && r < besti)) {
+              best = v;
+              besti = r;
+            }
+          }
+        }
+      }
+      // 2. The panel's interchanges as a permutation of the affected rows:
+      //    row aff_row[a] receives the old content of row aff_src[a].
+      if (tid == 0) {
+        int na = 0;
+        for (int kk = 0; kk < nbp; ++kk) {
+          const int k = k0 + kk, p = pivrow[k];
+          int ik = -1, ip = -1;
+          for (int u = 0; u < na; ++u) {
+            if (aff_row[u] == k) ik = u;
+            if (aff_row[u] == p) ip = u;
+          }
+          if (ik < 0) {
+            ik = na++;
+            aff_row[ik] = k;
+            aff_src[ik] = k;
+          }
+          if (ip < 0) {
+            ip = na++;
+            aff_row[ip] = p;
+            aff_src[ip] = p;
+          }
+          const int t = aff_src[ik];
+          aff_src[ik] = aff_src[ip];
+          aff_src[ip] = t;
+        }
+        s_na = na;
+      }
+      __syncthreads();
+      const int na = s_na;
+      const int oc = n - nbp;  // columns outside the panel
+      // In column blocks of CW: all affected rows of a column move within
+      // one block (read all, barrier, write all).
+      for (int cb = 0; cb < oc; cb += CW) {
+        z64 v[PV];
+#pragma unroll
+        for (int u = 0; u < PV; ++u) {
+          const int li = tid + u * T2;
+          const int aa = li / CW, cc = cb + li % CW;
+          if (aa < na && cc < oc) {
+            const int c = cc < k0 ? cc : cc + nbp;
+            v[u] = x[(int64_t)aff_src[aa] * ldx + c];
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < PV; ++u) {
+          const int li = tid + u * T2;
+          const int aa = li / CW, cc = cb + li % CW;
+          if (aa < na && cc < oc) {
+            const int c = cc < k0 ? cc : cc + nbp;
+            x[(int64_t)aff_row[aa] * ldx + c] = v[u];
+          }
+        }
+        __syncthreads();
+      }
+      // 3. Pivot rows (other columns) into Y.
+      const int ny = YS - 2;  // columns of whole tiles; those >= n stay zero
+      for (int idx = tid; idx < NB * ny; idx += T2) {
+        const int kk = idx / ny, c = idx % ny;
+        Y[kk * YS + c] = (kk < nbp && c < n && (c < k0 || c >= k0 + nbp)) ? x[(int64_t)(k0 + kk) * ldx + c]
+                                                                          : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+      // 4. Trailing update, one 16-row slice per warp at a time, no barriers.
+      const int mtiles = (n + 15) / 16;
+      for (int mt = warp; mt < mtiles; mt += W2) {
+        const int r0 = mt * 16;
+        // A fragments of this slice for all k (the panel transform rows).
+        for (int j0 = 0; j0 < n; j0 += 8 * JN) {
+          if (j0 >= k0 && j0 + 8 * JN <= k0 + nbp) continue;  // inside the panel
+          double cre[JN][4], cim[JN][4];
+#pragma unroll
+          for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int r = r0 + g + ((q >> 1) << 3);
+              const int c = j0 + j * 8 + 2 * tq + (q & 1);
+              z64 v = make_double2(0.0, 0.0);
+              if (r < n && c < n && !(r >= k0 && r < k0 + nbp) && (c < k0 || c >= k0 + nbp))
+                v = x[(int64_t)r * ldx + c];
+              cre[j][q] = v.x;
+              cim[j][q] = v.y;
+            }
+#pragma unroll
+          for (int k4 = 0; k4 < NB; k4 += 4) {
+            const int ra = r0 + g;
+            const z64 v0 = (ra < n) ? P[ra * PS + k4 + tq] : make_double2(0.0, 0.0);
+            const z64 v1 = (ra + 8 < n) ? P[(ra + 8) * PS + k4 + tq] : make_double2(0.0, 0.0);
+            const double nai0 = -v0.y, nai1 = -v1.y;
+            double br[JN], bi[JN];
+#pragma unroll
+            for (int j = 0; j < JN; ++j) {
+              const z64 bv = Y[(k4 + tq) * YS + j0 + j * 8 + g];
+              br[j] = bv.x;
+              bi[j] = bv.y;
+            }
+#pragma unroll
+            for (int j = 0; j < JN; ++j) {
+              mma_f64(cre[j], v0.x, v1.x, br[j]);
+              mma_f64(cim[j], v0.x, v1.x, bi[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < JN; ++j) {
+              mma_f64(cre[j], nai0, nai1, bi[j]);
+              mma_f64(cim[j], v0.y, v1.y, br[j]);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < JN; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int r = r0 + g + ((q >> 1) << 3);
+              const int c = j0 + j * 8 + 2 * tq + (q & 1);
+              if (r < n && c < n && (c < k0 || c >= k0 + nbp))
+                x[(int64_t)r * ldx + c] = make_double2(cre[j][q], cim[j][q]);
+            }
+        }
+      }
+      __syncthreads();
+      // 5. The panel transform back into X[:, K].
+      for (int idx = tid; idx < n * nbp; idx += T2) {
+        const int r = idx / nbp, c = idx % nbp;
+        x[(int64_t)r * ldx + k0 + c] = P[r * PS + c];
+      }
+      __syncthreads();
+    }
+
+    // Undo the column permutation: swaps applied from the last pivot back.
+    if (tid == 0) {
+      for (int c = 0; c < n; ++c) colsrc[c] = c;
+      for (int k = n - 1; k >= 0; --k) {
+        const int p = pivrow[k];
+        if (p != k) {
+          const int t = colsrc[k];
+          colsrc[k] = colsrc[p];
+          colsrc[p] = t;
+        }
+      }
+    }
+    __syncthreads();
+    // Row-wise gather through the (now free) panel buffer: PS rows fit.
+    const int nbufs = PS < W2 ? PS : W2;
+    if (warp < nbufs) {
+      z64* rowbuf = P + (size_t)warp * n;
+      for (int r = warp; r < n; r += nbufs) {
+        for (int c = lane; c < n; c += 32) rowbuf[c] = x[(int64_t)r * ldx + colsrc[c]];
+        __syncwarp();
+        for (int c = lane; c < n; c += 32) x[(int64_t)r * ldx + c] = rowbuf[c];
+        __syncwarp();
+      }
+    }
+    if (tid == 0 && info != nullptr && singular_at != 0 && info[b] == 0) info[b] = singular_at;
+    __syncthreads();
+  }
+}
+
+template <int NB>
+int launch2(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s) {
+  const size_t smem = Smem2<NB>::bytes(n);
+  if (smem > 227 * 1024) {
+    set_error("zinv: block size too large for the shared-memory panel");
+    return QTX_ERR_UNSUPPORTED;
+  }
+  QTX_CHECK_CUDA(
+      cudaFuncSetAttribute(zinv2_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned grid = (unsigned)(batch < 1048576 ? batch : 1048576);
+  ProfScope prof(QTX_KERNEL_ZINV, 8.0 * (double)n * n * n * (double)batch, s);
+  zinv2_kernel<NB><<<grid, T2, smem, s>>>(n, batch, A, X, info, active);
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
 }  // namespace
 
 int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s) {
@@ -362,7 +690,8 @@ int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active,
     set_error("zinv: null matrix");
     return QTX_ERR_ARG;
   }
-  if (n <= 512) return launch<16>(n, batch, A, X, info, active, s);
+  if (n <= 400) return launch2<16>(n, batch, A, X, info, active, s);
+  if (n <= 720) return launch2<8>(n, batch, A, X, info, active, s);
   if (n <= 1024) return launch<8>(n, batch, A, X, info, active, s);
   set_error("zinv: block sizes above 1024 are not supported");
   return QTX_ERR_UNSUPPORTED;
