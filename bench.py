@@ -46,7 +46,9 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=148)
     p.add_argument("--energies", type=int, default=1024)
-    p.add_argument("--e2e-batch", type=int, default=8)
+    p.add_argument("--e2e-batch", type=int, default=32, help="energies per end-to-end step (host memory: "
+                   "six pinned block-tridiagonal stacks of this many energies)")
+    p.add_argument("--e2e-subbatch", type=int, default=8, help="RGF max_batch_size of the end-to-end leg")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-energies", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
@@ -240,7 +242,7 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------------------
-def e2e_leg(torch, device, dev, energies, steps):
+def e2e_leg(torch, device, dev, energies, steps, sub=8):
     """The reference-facing plugin path with pinned HOST buffers: the caller's
     DSDBCOO stacks live in host memory; OBCSystem(SanchoRubio) and
     RGF.selected_solve copy them in and the results out in every step."""
@@ -275,7 +277,7 @@ def e2e_leg(torch, device, dev, energies, steps):
             A.blocks[i + 1, i] = torch.from_numpy(lower[i])
     fl, fr = dev.fermi_left(energies), dev.fermi_right(energies)
     obc_sys = OBCSystem(SanchoRubio(convergence_tol=1e-12, per_energy=True), memoization_mode="off")
-    solver = RGF(max_batch_size=B)
+    solver = RGF(max_batch_size=min(sub, B))
 
     def step():
         ob = OBCBlocks(n)
@@ -302,7 +304,7 @@ def e2e_leg(torch, device, dev, energies, steps):
     d2h = 3 * B * proto.nnz * elem + B * (n + 1) * elem + 6 * B * b * b * elem
     return {"value": steps * B / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "path": "RGF.selected_solve + OBCSystem(SanchoRubio) + contact_self_energy on pinned host DSDBCOO "
-                    f"stacks, {B} energies per step, {steps} steps"}
+                    f"stacks, {B} energies per step (RGF max_batch_size {min(sub, B)}), {steps} steps"}
 
 
 def run_ours(args, world, rank, local):
@@ -417,7 +419,9 @@ def run_ours(args, world, rank, local):
                          "peak_source": "measured cuBLAS FP32 GEMM with TF32 tensor cores 8192^3 on this GPU",
                          "launches": cg_n, "avg_launch_ms": cg_ms / cg_n if cg_n else None,
                          "share_of_step_time": cg_ms / mms if mms else None,
-                         "zinv_ms_share": mprof["zinv"][0] / mms if mms else None},
+                         "zinv_ms_share": mprof["zinv"][0] / mms if mms else None,
+                         "class_shares": {k: round(v[0] / mms, 4) for k, v in mprof.items()
+                                          if k != "all" and mms}},
             "error_vs_fp64": {"transmission_max_rel": float(terr.max()),
                               "transmission_median_rel": float(np.median(terr)),
                               "density_rel": float(np.linalg.norm(mprobe[1] - fprobe[1]) / np.linalg.norm(fprobe[1])),
@@ -430,7 +434,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1:
         if not args.no_e2e:
             e2e = e2e_leg(torch, device, dev, dev.energies[np.linspace(0, args.energies - 1, args.e2e_batch)
-                                                               .astype(int)], args.e2e_steps)
+                                                               .astype(int)], args.e2e_steps, args.e2e_subbatch)
         if not args.no_cpu:
             cpu = cpu_baseline(args.cpu_energies)
     if world > 1:
@@ -455,7 +459,8 @@ def run_ours(args, world, rank, local):
                     "traffic": None, "launches": gemm_n}
     roofline.update({"avg_launch_ms": gemm_ms / gemm_n if gemm_n else None,
                      "share_of_step_time": gemm_ms / ms if ms else None,
-                     "zinv_ms_share": inv_ms / ms if ms else None})
+                     "zinv_ms_share": inv_ms / ms if ms else None,
+                     "class_shares": {k: round(v[0] / ms, 4) for k, v in prof.items() if k != "all" and ms}})
     from quatrex_b200.negf import flops_per_energy
 
     its = np.mean(np.array(sr_iters), axis=0) if sr_iters else (0, 0)

@@ -231,9 +231,16 @@ class BTView:
         nnz = int(src.shape[-1])
         self.lead_shape = lead
         k = kind(src)
-        if self.role == "in" or k in ("torch", "cupy"):
+        host = k == "numpy" or (k == "torch" and src.device.type == "cpu")
+        self._host = host
+        self._need = need
+        # Inputs cross the bus as one contiguous copy (a DMA at full link
+        # speed; per-block strided copies would be staged through pageable
+        # memory).
+        if self.role == "in" or (k in ("torch", "cupy") and not host):
             t = to_device(src, self.device)
         else:
+            # host output: nothing is uploaded; finalize() returns the written blocks
             t = torch.zeros(src.shape, dtype=_C128, device=self.device)
         t2 = t.reshape(-1, nnz) if t.numel() else t.reshape(0, nnz)
         if self.role == "out" and k in ("torch", "cupy") and t2.data_ptr() != t.data_ptr():
@@ -316,6 +323,38 @@ class BTView:
         self._l = (QtxMat * max(n - 1, 1))(*(self.lower or [NULL_MAT]))
         return _native.QtxBT(n, self._bs, self._d, self._u, self._l)
 
+    def can_finalize_async(self) -> bool:
+        """True when finalize_async() applies: a block-sorted COO host
+        container whose blocks are all dense in place (no sparsify pass)."""
+        return (self.role == "out" and self.layout is not None and not self.pending
+                and getattr(self, "_host", False) and kind(self.m.data) == "torch")
+
+    def finalize_async(self, write_lower: bool = True) -> None:
+        """finalize() without synchronising: the device-to-host copies of the
+        written blocks are enqueued on the current stream; the caller keeps
+        this view alive, synchronises, then calls the returned callable (if
+        any) before reading the container."""
+        written = [e for (i, j), e in self.layout.entries.items() if e is not None and (
+            (i == j and "diag" in self._need) or (j == i + 1 and "upper" in self._need)
+            or (j == i - 1 and "lower" in self._need and write_lower))]
+        total = sum(e is not None for e in self.layout.entries.values())
+        dst = self.m.data[self.sl]
+        src = self.data.reshape(self.data_src.shape)
+        if len(written) == total:
+            dst.copy_(src, non_blocking=True)
+            return None
+        # Some blocks must keep the container's values: one contiguous DMA
+        # into pinned staging now, the written ranges copied on the host by
+        # the returned callable once the stream has been synchronised.
+        stage = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+        stage.copy_(src, non_blocking=True)
+
+        def scatter():
+            for e in written:
+                dst[..., e.start:e.stop] = stage[..., e.start:e.stop]
+
+        return scatter
+
     def finalize(self, write_lower: bool = True) -> None:
         """Writes results back to the container (role "out")."""
         if self.role != "out":
@@ -331,8 +370,24 @@ class BTView:
                     self.batch, mat(dense), e.stop - e.start, rows.data_ptr(), cols.data_ptr(),
                     self.data.data_ptr() + e.start * _ELEM, self.data.stride(0), self.stream))
             if not self._inplace_out:
-                torch.cuda.current_stream(self.device).synchronize()
-                assign(self.m.data[self.sl], self.data.reshape(self.data_src.shape))
+                written = [e for (i, j), e in self.layout.entries.items() if e is not None and (
+                    (i == j and "diag" in self._need) or (j == i + 1 and "upper" in self._need)
+                    or (j == i - 1 and "lower" in self._need and write_lower))]
+                total = sum(e is not None for e in self.layout.entries.values())
+                if self._host and len(written) < total:
+                    # only the blocks the solver wrote go back to the host container
+                    dst = self.m.data[self.sl]
+                    hd = dst if kind(dst) == "torch" else None
+                    src = self.data.reshape(self.data_src.shape)
+                    for e in written:
+                        if hd is not None:
+                            hd[..., e.start:e.stop].copy_(src[..., e.start:e.stop], non_blocking=True)
+                        else:
+                            dst[..., e.start:e.stop] = src[..., e.start:e.stop].cpu().numpy()
+                    torch.cuda.current_stream(self.device).synchronize()
+                else:
+                    torch.cuda.current_stream(self.device).synchronize()
+                    assign(self.m.data[self.sl], self.data.reshape(self.data_src.shape))
             return
         torch.cuda.current_stream(self.device).synchronize()
         stack = self._stack_view

@@ -136,6 +136,10 @@ class RGF(GFSolver):
             current = _zeros_like_array(sigma_lesser.data, cshape)
 
         sizes, slices = get_batches(sigma_lesser.shape[0], self.max_batch_size)
+        if len(sizes) > 1 and all(_on_host(m) for m in (a, sigma_lesser, sigma_greater, xl, xg)):
+            return self._selected_solve_pipelined(a, sigma_lesser, sigma_greater, obc_blocks, xl, xg, xr,
+                                                  current, sizes, slices, out, return_retarded,
+                                                  return_current)
         st = _stream(device)
         for b in range(len(sizes)):
             sl = slice(int(slices[b]), int(slices[b + 1]), 1)
@@ -180,6 +184,99 @@ class RGF(GFSolver):
         if return_current:
             return current
         return None
+
+    def _selected_solve_pipelined(self, a, sigma_lesser, sigma_greater, obc_blocks, xl, xg, xr, current, sizes,
+                                  slices, out, return_retarded, return_current):
+        """selected_solve for host (CPU torch) containers with more than one
+        batch: batch k+1 is uploaded on a copy stream and batch k-1 written
+        back on a third stream while batch k is solved. Same results and
+        conventions; a singular block raises after the last batch."""
+        lib = _native.load()
+        device = self._dev()
+        n = int(sigma_lesser.num_blocks)
+        comp = torch.cuda.current_stream(device)
+        up_s, down_s = torch.cuda.Stream(device), torch.cuda.Stream(device)
+        sym_l = bool(getattr(xl, "symmetry", False))
+        sym_g = bool(getattr(xg, "symmetry", False))
+        flags = _native.QTX_SOLVE_SYMMETRIC_OUT if (sym_l or sym_g) else 0
+        keep, infos, curs, deferred = [], [], [], []
+
+        def stage(b):
+            sl = slice(int(slices[b]), int(slices[b + 1]), 1)
+            with torch.cuda.stream(up_s):
+                hs = up_s.cuda_stream
+                views = (BTView(a, sl, device, hs, "in"),
+                         BTView(sigma_lesser, sl, device, hs, "in", need=("diag", "upper")),
+                         BTView(sigma_greater, sl, device, hs, "in", need=("diag", "upper")),
+                         BTView(xl, sl, device, hs, "out"), BTView(xg, sl, device, hs, "out"),
+                         BTView(xr, sl, device, hs, "out", need=("diag",)) if xr is not None else None)
+                obc_keep: list = []
+                obcs = (obc_mats(obc_blocks.retarded, sl, n, device, obc_keep),
+                        obc_mats(obc_blocks.lesser, sl, n, device, obc_keep),
+                        obc_mats(obc_blocks.greater, sl, n, device, obc_keep))
+                ev = torch.cuda.Event()
+                ev.record(up_s)
+            return sl, views, obcs, obc_keep, ev
+
+        nxt = stage(0)
+        for b in range(len(sizes)):
+            sl, views, obcs, obc_keep, ev = nxt
+            comp.wait_event(ev)
+            if b + 1 < len(sizes):
+                nxt = stage(b + 1)
+            A, SL, SG, XL, XG, XR = views
+            batch = A.batch
+            cur = torch.zeros((batch, n + 1), dtype=torch.complex128, device=device) if return_current else None
+            abi = [v.abi() if v is not None else None for v in views]
+            ws_bytes = lib.qtx_selected_solve_workspace(n, abi[0].block_sizes, batch, int(return_current))
+            ws = workspace_pool.get(ws_bytes, device, "rgf")
+            info = torch.zeros(batch, dtype=torch.int32, device=device)
+            _native.check(lib.qtx_selected_solve(
+                ctypes.byref(abi[0]), ctypes.byref(abi[1]), ctypes.byref(abi[2]), obcs[0], obcs[1], obcs[2],
+                ctypes.byref(abi[3]), ctypes.byref(abi[4]),
+                ctypes.byref(abi[5]) if abi[5] is not None else None,
+                cur.data_ptr() if cur is not None else None, NULL_MAT, None, flags, batch,
+                info.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.c_void_p(comp.cuda_stream)))
+            done = torch.cuda.Event()
+            done.record(comp)
+            with torch.cuda.stream(down_s):
+                down_s.wait_event(done)
+                for v, lower in ((XL, not sym_l), (XG, not sym_g), (XR, True)):
+                    if v is None:
+                        continue
+                    if v.can_finalize_async():
+                        post = v.finalize_async(write_lower=lower)
+                        if post is not None:
+                            deferred.append(post)
+                    else:
+                        down_s.synchronize()
+                        v.finalize(write_lower=lower)
+            keep.append((views, obc_keep, abi))
+            infos.append(info)
+            curs.append((sl, cur))
+        down_s.synchronize()
+        comp.synchronize()
+        for post in deferred:
+            post()
+        for info in infos:
+            _raise_if_singular(info)
+        if return_current:
+            for sl, cur in curs:
+                _assign_rows(current, sl, cur)
+        if out is None:
+            if return_retarded:
+                if return_current:
+                    return xl, xg, xr, current
+                return xl, xg, xr
+            return xl, xg
+        if return_current:
+            return current
+        return None
+
+
+def _on_host(m) -> bool:
+    d = getattr(m, "data", None)
+    return isinstance(d, torch.Tensor) and d.device.type == "cpu"
 
 
 def _zeros_like_array(like, shape):
