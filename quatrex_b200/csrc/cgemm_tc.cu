@@ -164,8 +164,10 @@ __device__ __forceinline__ void b_task(int t, int& row, int& chunk) {
   }
 }
 
-// Global -> registers for one K block (all loads issued back to back).
-template <int OPA, int OPB>
+// Global -> registers for one K block (all loads issued back to back). With
+// VEC (operands 16-byte aligned, even leading dimensions) the K-contiguous
+// operands are read two complex numbers per 16-byte load.
+template <int OPA, int OPB, bool VEC>
 __device__ __forceinline__ void load_regs(const Args& a, const c32* Ag, const c32* Bg, Regs& R, int m0,
                                           int n0, int k0, int tid) {
 #pragma unroll
@@ -173,6 +175,22 @@ __device__ __forceinline__ void load_regs(const Args& a, const c32* Ag, const c3
     int row, chunk;
     a_task<OPA>(tid + i * THREADS, row, chunk);
     const int gr = m0 + row;
+    if (OPA == 0 && VEC) {
+#pragma unroll
+      for (int e = 0; e < 4; e += 2) {
+        const int gk = k0 + chunk * 4 + e;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gr < a.M && gk + 1 < a.K) {
+          v = *reinterpret_cast<const float4*>(Ag + (int64_t)gr * a.A.ld + gk);
+        } else if (gr < a.M && gk < a.K) {
+          const float2 w = Ag[(int64_t)gr * a.A.ld + gk];
+          v = make_float4(w.x, w.y, 0.f, 0.f);
+        }
+        R.a[i][e] = make_float2(v.x, v.y);
+        R.a[i][e + 1] = make_float2(v.z, v.w);
+      }
+      continue;
+    }
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int gk = k0 + chunk * 4 + e;
@@ -193,6 +211,22 @@ __device__ __forceinline__ void load_regs(const Args& a, const c32* Ag, const c3
     int row, chunk;
     b_task<OPB>(tid + i * THREADS, row, chunk);
     const int gn = n0 + row;
+    if (OPB == 1 && VEC) {
+#pragma unroll
+      for (int e = 0; e < 4; e += 2) {
+        const int gk = k0 + chunk * 4 + e;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gn < a.N && gk + 1 < a.K) {
+          v = *reinterpret_cast<const float4*>(Bg + (int64_t)gn * a.B.ld + gk);
+        } else if (gn < a.N && gk < a.K) {
+          const float2 w = Bg[(int64_t)gn * a.B.ld + gk];
+          v = make_float4(w.x, w.y, 0.f, 0.f);
+        }
+        R.b[i][e] = make_float2(v.x, -v.y);
+        R.b[i][e + 1] = make_float2(v.z, -v.w);
+      }
+      continue;
+    }
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int gk = k0 + chunk * 4 + e;
@@ -289,7 +323,7 @@ __device__ __forceinline__ float2 addend_at(const Args& a, int t, int64_t b, int
   return cmulf(ad.coef, x);
 }
 
-template <int OPA, int OPB>
+template <int OPA, int OPB, bool VEC>
 __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Args a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the SWIZZLE_128B atoms.
@@ -332,7 +366,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Ar
     const c32* Ag = at<const c32>(a.A, b);
     const c32* Bg = at<const c32>(a.B, b);
     if (KB > 0) {
-      load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, 0, tid);
+      load_regs<OPA, OPB, VEC>(a, Ag, Bg, R, m0, n0, 0, tid);
       store_planes<OPA, OPB>(R, planes, tid);
       fence_async_smem();
       __syncthreads();
@@ -347,7 +381,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Ar
         mma_commit(bar);
       }
       const bool more = kb + 1 < KB;
-      if (more) load_regs<OPA, OPB>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
+      if (more) load_regs<OPA, OPB, VEC>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
       if (!mbar_wait(bar, phase)) ok = false;
       phase ^= 1u;
       if (more && ok) {
@@ -456,17 +490,30 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Ar
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-template <int OPA, int OPB>
-int launch(const Args& a, cudaStream_t s) {
+template <int OPA, int OPB, bool VEC>
+int launch_v(const Args& a, cudaStream_t s) {
   static_assert(TM * S_LD * (int)sizeof(float2) <= PLANES_BYTES, "epilogue tile must fit the planes");
   const size_t smem = (size_t)PLANES_BYTES + 64 + 1024;
-  QTX_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<OPA, OPB>,
+  QTX_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel<OPA, OPB, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((a.N + TN - 1) / TN, (a.M + TM - 1) / TM, (unsigned)(a.batch < 65535 ? a.batch : 65535));
   ProfScope prof(QTX_KERNEL_CGEMM, 8.0 * a.M * a.N * (double)a.K * (double)a.batch, s);
-  cgemm_tc_kernel<OPA, OPB><<<grid, THREADS, smem, s>>>(a);
+  cgemm_tc_kernel<OPA, OPB, VEC><<<grid, THREADS, smem, s>>>(a);
   QTX_CHECK_LAUNCH();
   return QTX_OK;
+}
+
+bool vec_ok(const MatRef& m) {
+  return (reinterpret_cast<uintptr_t>(m.p) & 15u) == 0 && (m.ld % 2) == 0 && (m.stride % 2) == 0;
+}
+
+template <int OPA, int OPB>
+int launch(const Args& a, cudaStream_t s) {
+  // The 16-byte path reads the K-contiguous operands; both must allow it.
+  const bool va = OPA != 0 || vec_ok(a.A);
+  const bool vb = OPB != 1 || vec_ok(a.B);
+  if (va && vb) return launch_v<OPA, OPB, true>(a, s);
+  return launch_v<OPA, OPB, false>(a, s);
 }
 
 }  // namespace
