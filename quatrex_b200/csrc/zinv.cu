@@ -372,8 +372,7 @@ int launch(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* activ
 constexpr int T2 = 512;
 constexpr int W2 = T2 / 32;
 constexpr int JN = 2;    // n8 tiles per column tile of the trailing update
-constexpr int CW = 128;  // column block of the row-interchange pass
-constexpr int PV = 8;    // its elements per thread: 2 NB rows x CW columns <= T2 x PV for NB <= 16
+constexpr int PV = 8;  // elements per thread of one row-interchange block
 
 template <int NB>
 struct Smem2 {
@@ -395,7 +394,10 @@ template <int NB>
 __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatRef A, MatRef X, int* info,
                                                       const int* active) {
   using S = Smem2<NB>;
-  static_assert(2 * NB * CW <= T2 * PV, "interchange block must fit the per-thread registers");
+  // Column block of the row-interchange pass: all 2 NB affected rows of CW
+  // columns fit T2 x PV registers.
+  constexpr int CW = (T2 * PV) / (2 * NB);
+  static_assert(NB % 4 == 0 && 2 * NB * CW <= T2 * PV, "panel width and interchange block");
   constexpr int PS = S::PS;
   const int YS = S::ys(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
