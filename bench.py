@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--cfg4-rate", type=float, default=None,
                    help="arrivals per second (default: 0.7 of the measured capacity)")
     p.add_argument("--cfg4-duration", type=float, default=60.0)
+    p.add_argument("--graph", action="store_true",
+                   help="replay each batch through one captured CUDA graph (device-side Sancho-Rubio loop)")
     p.add_argument("--inverse-path", choices=["auto", "single", "wide"], default="auto",
                    help="inverse kernels: automatic choice, one CTA per matrix, or multi-CTA panels")
     return p.parse_args()
@@ -337,10 +339,12 @@ def run_ours(args, world, rank, local):
 
     def timed(precision):
         solver = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True,
-                                   device=device, precision=precision)
+                                   device=device, precision=precision, device_loop=args.graph)
 
         def step(k):
             idx = batches[k % len(batches)]
+            if args.graph:
+                return solver.solve_graph(dev.energies[idx], fl_all[idx], fr_all[idx])
             return solver.solve(dev.energies[idx], fl_all[idx], fr_all[idx])
 
         for k in range(args.warmup):
@@ -356,19 +360,40 @@ def run_ours(args, world, rank, local):
         clocks.start()
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         t_start.record()
         for k in range(args.steps):
             r = step(args.warmup + k)
-            sr_iters.append(r.sr_iterations)
+            if not args.graph:
+                sr_iters.append(r.sr_iterations)
+            marks[k].record()
         t_end.record()
         torch.cuda.synchronize()
+        per_step = [t_start.elapsed_time(marks[0])] + [marks[k - 1].elapsed_time(marks[k])
+                                                         for k in range(1, args.steps)]
+        if args.graph:
+            # graph replays record no per-launch profile: one eager step after
+            # the timed region gives the kernel-class breakdown
+            it = solver.sr_status(B)[0]
+            sr_iters = [(it, it)] * args.steps
+            lib.qtx_profile_reset()
+            t_a = torch.cuda.Event(enable_timing=True)
+            t_b = torch.cuda.Event(enable_timing=True)
+            t_a.record()
+            idx = batches[0]
+            solver.solve(dev.energies[idx], fl_all[idx], fr_all[idx])
+            t_b.record()
+            torch.cuda.synchronize()
+            prof_ms = t_a.elapsed_time(t_b)
         if world > 1:
             dist.barrier()
         clk = clocks.stop()
         lib.qtx_profile_enable(0)
         ms = t_start.elapsed_time(t_end)
+        prof_ref_ms = prof_ms if args.graph else ms  # the time the launch profile covers
         prof = {name: _native.profile_read(kind) for name, kind in _native.KERNEL_CLASSES.items()}
         prof["all"] = _native.profile_read(-1)
+
         lib.qtx_profile_reset()
         # a fixed probe batch for cross-precision error reporting
         probe = batches[0]
@@ -377,13 +402,13 @@ def run_ours(args, world, rank, local):
         probe_out = (rp.transmission.cpu().numpy().copy(), rp.density.cpu().numpy().copy())
         del solver
         torch.cuda.empty_cache()
-        return ms, prof, clk, sr_iters, probe_out
+        return ms, prof, clk, sr_iters, probe_out, per_step, prof_ref_ms
 
     res = {}
     for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
         res[prec] = timed(prec)
     main_prec = "fp64" if "fp64" in res else "mixed"
-    ms, prof, clk, sr_iters, _ = res[main_prec]
+    ms, prof, clk, sr_iters, _, per_step, pms = res[main_prec]
     gemm_ms, gemm_flops, gemm_n = prof["zgemm"] if main_prec == "fp64" else prof["cgemm"]
     inv_ms, inv_flops, inv_n = prof["zinv"]
     all_ms, _, all_n = prof["all"]
@@ -400,7 +425,7 @@ def run_ours(args, world, rank, local):
 
     mixed_line = None
     if "mixed" in res and main_prec == "fp64":
-        mms, mprof, mclk, _, mprobe = res["mixed"]
+        mms, mprof, mclk, _, mprobe, mper, mpms = res["mixed"]
         tm = torch.tensor([mms], dtype=torch.float64, device=device)
         if world > 1:
             dist.all_reduce(tm, op=dist.ReduceOp.MAX)
@@ -418,15 +443,16 @@ def run_ours(args, world, rank, local):
                          "frac": (ach / tf32_peak) if (ach and tf32_peak) else None,
                          "peak_source": "measured cuBLAS FP32 GEMM with TF32 tensor cores 8192^3 on this GPU",
                          "launches": cg_n, "avg_launch_ms": cg_ms / cg_n if cg_n else None,
-                         "share_of_step_time": cg_ms / mms if mms else None,
-                         "zinv_ms_share": mprof["zinv"][0] / mms if mms else None,
-                         "class_shares": {k: round(v[0] / mms, 4) for k, v in mprof.items()
-                                          if k != "all" and mms}},
+                         "share_of_step_time": cg_ms / mpms if mpms else None,
+                         "zinv_ms_share": mprof["zinv"][0] / mpms if mpms else None,
+                         "class_shares": {k: round(v[0] / mpms, 4) for k, v in mprof.items()
+                                          if k != "all" and mpms}},
             "error_vs_fp64": {"transmission_max_rel": float(terr.max()),
                               "transmission_median_rel": float(np.median(terr)),
                               "density_rel": float(np.linalg.norm(mprobe[1] - fprobe[1]) / np.linalg.norm(fprobe[1])),
                               "probe": f"{batches[0].size} energies of the grid"},
-            "gpu_launches": mprof["all"][2], "clocks": mclk,
+            "gpu_launches": mprof["all"][2] * (args.steps if args.graph else 1), "clocks": mclk,
+            "latency_ms": _latency(mper, B),
         }
 
     e2e = None
@@ -458,9 +484,11 @@ def run_ours(args, world, rank, local):
                     "peak_source": "measured cuBLAS FP32 GEMM with TF32 tensor cores 8192^3 on this GPU",
                     "traffic": None, "launches": gemm_n}
     roofline.update({"avg_launch_ms": gemm_ms / gemm_n if gemm_n else None,
-                     "share_of_step_time": gemm_ms / ms if ms else None,
-                     "zinv_ms_share": inv_ms / ms if ms else None,
-                     "class_shares": {k: round(v[0] / ms, 4) for k, v in prof.items() if k != "all" and ms}})
+                     "share_of_step_time": gemm_ms / pms if pms else None,
+                     "zinv_ms_share": inv_ms / pms if pms else None,
+                     "class_shares": {k: round(v[0] / pms, 4) for k, v in prof.items() if k != "all" and pms},
+                     "profiled": "the timed steps" if not args.graph else
+                                 "one eager step after the timed graph replays"})
     from quatrex_b200.negf import flops_per_energy
 
     its = np.mean(np.array(sr_iters), axis=0) if sr_iters else (0, 0)
@@ -480,11 +508,20 @@ def run_ours(args, world, rank, local):
         "as_written_tflops": value * fl["total"] / 1e12,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": all_n,
+        "gpu_launches": all_n * (args.steps if args.graph else 1),
         "clocks": clk,
+        "latency_ms": _latency(per_step, B),
         "mixed": mixed_line,
     }
     print(json.dumps(line), flush=True)
+
+
+def _latency(per_step, batch) -> dict:
+    """Solve latency of one batch (device time between consecutive step
+    ends on the solving stream)."""
+    x = np.asarray(per_step, dtype=np.float64)
+    return {"p50": float(np.percentile(x, 50)), "p99": float(np.percentile(x, 99)), "max": float(x.max()),
+            "batch": int(batch), "samples": int(x.size), "unit": "ms per batch"}
 
 
 def _ncu_traffic():
