@@ -65,8 +65,10 @@ def parse():
                    help="serving catalogue: 8 devices with (N, b) drawn as in cfg3 with b in {128, 256} "
                         "(small) or b in {128, ..., 768} (cfg3)")
     p.add_argument("--cfg4-rate", type=float, default=None,
-                   help="arrivals per second (default: 0.7 of the measured capacity)")
+                   help="arrivals per second (default: --cfg4-load of the measured capacity)")
     p.add_argument("--cfg4-duration", type=float, default=60.0)
+    p.add_argument("--cfg4-load", type=float, default=0.5,
+                   help="arrival rate as a fraction of the capacity measured per lane")
     p.add_argument("--graph", action="store_true",
                    help="replay each batch through one captured CUDA graph (device-side Sancho-Rubio loop)")
     p.add_argument("--inverse-path", choices=["auto", "single", "wide"], default="auto",
@@ -639,8 +641,9 @@ def run_cfg3(args, local):
     res, obs = {}, {}
     precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     for prec in precs:
-        runner = UnevenBatchRunner(jobs, precision=prec, budget_bytes=args.budget_gb * 1e9, device=device)
-        runner.prepare()  # captures every device's graph (one eager pass each)
+        runner = UnevenBatchRunner(jobs, precision=prec, budget_bytes=args.budget_gb * 1e9, device=device,
+                                   autotune=True)
+        runner.prepare()  # tunes batch sizes, then captures every device's graph (one eager pass each)
         gpu = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
         clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
         clocks.start()
@@ -652,6 +655,7 @@ def run_cfg3(args, local):
         sec = t0.elapsed_time(t1) * 1e-3
         res[prec] = {"value": len(jobs) * ne / sec, "seconds": sec, "as_written_tflops": work / sec / 1e12,
                      "devices": runner.summary(), "sr_converged": all(runner.sr_converged().values()),
+                     "tuning": runner.tuning,
                      "clocks": clocks.stop()}
         obs[prec] = {k: v["transmission"].cpu().numpy().copy() for k, v in runner.results().items()}
         del runner
@@ -682,7 +686,7 @@ def run_cfg4(args, local):
 
     from quatrex_b200 import synthetic
     from quatrex_b200.negf import flops_per_energy
-    from quatrex_b200.serving import EnergyServer, poisson_requests
+    from quatrex_b200.serving import EnergyServer, Request, latency_stats, poisson_requests, slowdown_stats
     from quatrex_b200.uneven import jobs_from_devices
 
     device = torch.device("cuda", local)
@@ -702,7 +706,7 @@ def run_cfg4(args, local):
     for prec in precs:
         srv = EnergyServer(cat, precision=prec, budget_bytes=args.budget_gb * 1e9, warm_start=True,
                            device=device)
-        if rate is None:  # 0.7 of the capacity measured on one cold replay per lane, lanes run back to back
+        if rate is None:  # a fraction of the capacity measured on one cold replay per lane, lanes back to back
             per_energy = []
             for ln in srv.lanes:
                 t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -712,13 +716,30 @@ def run_cfg4(args, local):
                     t1.record()
                 torch.cuda.synchronize()
                 per_energy.append(t0.elapsed_time(t1) * 1e-3 / ln.B)
-            rate = 0.7 / (mean_n * float(np.mean(per_energy)))
+            rate = args.cfg4_load / (mean_n * float(np.mean(per_energy)))
         reqs = poisson_requests(rate, args.cfg4_duration, [grid] * len(cat), (64, 512), seed=0)
         gpu = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
         clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
         clocks.start()
         stats = srv.run(reqs)
         stats["clocks"] = clocks.stop()
+        mixed_lat = {r.rid: r.latency for r in reqs}
+        del srv
+        torch.cuda.empty_cache()
+        # Isolated solve time: each request served alone on an idle server
+        # with the same lanes and no warm starts.
+        solo = EnergyServer(cat, precision=prec, budget_bytes=args.budget_gb * 1e9, warm_start=False,
+                            device=device)
+        alone = {}
+        for r in reqs:
+            q = Request(r.rid, r.device, r.grid_index)
+            t0 = time.perf_counter()
+            solo.solve_now(q)
+            alone[r.rid] = time.perf_counter() - t0
+        stats["isolated_latency"] = latency_stats(list(alone.values()))
+        stats["slowdown_vs_isolated"] = slowdown_stats(mixed_lat, alone)
+        del solo
+        srv = None
         stats["as_written_tflops"] = stats["energies"] * req_flops / mean_n / stats["wall_s"] / 1e12
         out[prec] = stats
         del srv
@@ -731,10 +752,12 @@ def run_cfg4(args, local):
         "config": {"workload": f"Poisson arrivals at {rate:.3g} req/s for {args.cfg4_duration:g} s, seed 0; "
                                f"catalogue of 8 devices (N, b) = {shapes}, 512-point grids on [-2,2]; "
                                "64-512 grid energies per request",
-                   "rate_rule": "given" if args.cfg4_rate else "0.7 of the capacity measured per lane",
+                   "rate_rule": "given" if args.cfg4_rate else f"{args.cfg4_load} of the capacity measured per lane",
                    "budget_gb": args.budget_gb, "warm_starts": True,
                    "latency_clock": "host wall clock, arrival to completion"},
         "p50_s": main["latency"].get("p50_s"), "p99_s": main["latency"].get("p99_s"),
+        "p99_over_isolated_p99": (main["latency"].get("p99_s") / main["isolated_latency"]["p99_s"]
+                                  if main["isolated_latency"].get("p99_s") else None),
         "results": out,
         "offered_load_note": {
             "spec_rate_req_s": 200, "spec_mean_request_tflop": spec_req_flops / 1e12,

@@ -107,6 +107,16 @@ def form_batch(pending: deque, cached: np.ndarray, B: int) -> tuple[list, bool]:
     return take, warm
 
 
+def slowdown_stats(mixed: dict, alone: dict) -> dict:
+    """Per-request latency in the mix divided by the same request's latency
+    served alone on an idle server ({rid: seconds} each)."""
+    r = np.array([mixed[k] / alone[k] for k in mixed if k in alone and alone[k] > 0])
+    if r.size == 0:
+        return {"count": 0}
+    return {"count": int(r.size), "p50": float(np.percentile(r, 50)), "p99": float(np.percentile(r, 99)),
+            "max": float(r.max())}
+
+
 def latency_stats(latencies) -> dict:
     lat = np.asarray(latencies, dtype=np.float64)
     if lat.size == 0:

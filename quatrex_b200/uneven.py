@@ -224,7 +224,8 @@ class UnevenBatchRunner:
 
     def __init__(self, jobs: list[DeviceJob], precision: str = "fp64", budget_bytes: float = 150e9,
                  batches: list[int] | None = None, device: torch.device | None = None, sr_tol: float = 1e-12,
-                 sr_max_iterations: int = 100):
+                 sr_max_iterations: int = 100, autotune: bool = False, tuner: BatchTuner | None = None,
+                 max_trials: int = 3):
         self.jobs = list(jobs)
         self.precision = precision
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -237,10 +238,57 @@ class UnevenBatchRunner:
         self.sr_tol = sr_tol
         self.sr_max_iterations = sr_max_iterations
         self.states: list[JobState] = []
+        self.autotune = autotune
+        self.tuner = tuner or BatchTuner()
+        self.max_trials = max_trials
+        self.num_sms = num_sms
+        self.tuning: dict = {}
+
+    def _measure(self, job: DeviceJob, B: int) -> float:
+        """Seconds of one captured-graph replay of B energies of ``job``."""
+        dev = self.device
+        s = EnergyPointSolver(job.h_diag, job.coupling, eta=job.eta, sr_tol=self.sr_tol,
+                              sr_max_iterations=self.sr_max_iterations, per_energy=True, device=dev,
+                              precision=self.precision, device_loop=True, store_blocks=False)
+        idx = np.arange(B) % job.num_energies
+        E = torch.as_tensor(np.asarray(job.energies, dtype=np.float64)[idx], device=dev)
+        fl = torch.as_tensor(np.asarray(job.f_left, dtype=np.float64)[idx], device=dev)
+        fr = torch.as_tensor(np.asarray(job.f_right, dtype=np.float64)[idx], device=dev)
+        s.set_inputs_device(E, fl, fr)
+        g = s.capture(B)  # runs the pipeline once eagerly, then captures
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        g.replay()
+        t1.record()
+        torch.cuda.synchronize(dev)
+        sec = t0.elapsed_time(t1) * 1e-3
+        del g, s
+        torch.cuda.empty_cache()
+        return sec
+
+    def tune(self) -> None:
+        """Measured batch sizes: per (N, b) the largest ``max_trials`` rungs
+        of the ladder up to the planned (budget-feasible) batch are timed and
+        the one with the most energies per second is kept (cached per GPU
+        and shape in the BatchTuner)."""
+        gpu = torch.cuda.get_device_name(self.device)
+        for k, job in enumerate(self.jobs):
+            plan = self.batches[k]
+            cands = [c for c in batch_ladder(self.num_sms, plan)]
+            if plan not in cands:
+                cands.append(plan)
+            cands = sorted(set(cands))[-self.max_trials:]
+            key = BatchTuner.key(gpu, job.num_blocks, job.block_size, self.precision)
+            res = self.tuner.tune(key, cands, lambda B, j=job: self._measure(j, B))
+            self.tuning[job.name] = res
+            self.batches[k] = min(int(res["batch"]), plan)
 
     def prepare(self) -> None:
         """Allocates every solver and captures its graph (runs each pipeline
-        once eagerly). Nothing here belongs in a timed region."""
+        once eagerly), after tuning the batch sizes if asked. Nothing here
+        belongs in a timed region."""
+        if self.autotune and not self.tuning:
+            self.tune()
         dev = self.device
         for job, B in zip(self.jobs, self.batches):
             solver = EnergyPointSolver(job.h_diag, job.coupling, eta=job.eta, sr_tol=self.sr_tol,

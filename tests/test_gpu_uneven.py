@@ -45,3 +45,19 @@ def test_uneven_runner_replays_are_deterministic(cuda_device):
     b = {k: v["transmission"].cpu().numpy() for k, v in runner.results().items()}
     for k in a:
         np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_uneven_runner_autotune(cuda_device):
+    devs = [synthetic.make_device(4, 32, np.linspace(-1.5, 1.5, 12), seed=15),
+            synthetic.make_device(3, 48, np.linspace(-1.0, 1.0, 9), seed=16)]
+    jobs = jobs_from_devices(devs)
+    runner = UnevenBatchRunner(jobs, batches=[8, 9], budget_bytes=4e9, autotune=True, max_trials=2)
+    res = runner.run()
+    assert set(runner.tuning) == {j.name for j in jobs}
+    for j, cap in zip(jobs, (8, 9)):
+        t = runner.tuning[j.name]
+        assert 1 <= int(t["batch"]) <= cap and len(t["trials"]) >= 1
+    for d, j in zip(devs, jobs):
+        r = EnergyPointSolver(d.h_diag, d.coupling, eta=d.eta, sr_tol=1e-12, per_energy=True).solve(
+            d.energies, d.fermi_left(), d.fermi_right())
+        assert _rel(res[j.name]["transmission"].cpu().numpy(), r.transmission.cpu().numpy()) < 1e-10
