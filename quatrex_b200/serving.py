@@ -12,12 +12,17 @@ catalogue device resident on the GPU:
   only) with two captured CUDA graphs of one batch size: *cold* (both-contact
   Sancho-Rubio) and *warm* (the lane's resident surface Green's functions of
   the requested grid points, then the OBCSystem fixed-point step);
-* its own stream and pinned staging buffers for two batches in flight;
-* a FIFO of pending (request, energy) items. Whenever fewer than two
-  batches are in flight the lane launches the next batch from the FIFO,
-  items of different requests mixed (continuous batching): warm items
-  (grid points already solved once) go together in a warm batch, the rest in
-  a cold batch. One replay needs only the index vector as input.
+* two streams (low and high priority) and pinned staging buffers for two
+  batches in flight; a batch whose oldest request has at most the median
+  remaining work of all active requests goes to the high-priority stream
+  (shortest remaining work first across lanes), and a lane's batches stay
+  ordered through an event chain;
+* a queue of pending (request, energy) items, ordered by the requests'
+  remaining work (shortest first). Whenever fewer than two batches are in
+  flight the lane launches the next batch from the queue, items of
+  different requests mixed (continuous batching): warm items (grid points
+  already solved once) go together in a warm batch, the rest in a cold
+  batch. One replay needs only the index vector as input.
 
 Admission: at start-up every lane gets a batch size from
 :func:`quatrex_b200.uneven.plan_batches` such that all lanes, their graphs,
@@ -135,6 +140,12 @@ class _Lane:
         if warm_start:
             self.solver.enable_obc_cache()
         self.stream = torch.cuda.Stream(device)
+        # Two priorities for the shortest-remaining-work rule; a lane's
+        # batches stay ordered through `last` whichever stream they use.
+        lo, hi = torch.cuda.Stream.priority_range()
+        self.streams = {False: torch.cuda.Stream(device, priority=lo), True: torch.cuda.Stream(device, priority=hi)}
+        self.last = None
+        self.urgent_batches = 0
         G = job.num_energies
         self.cached = np.zeros(G, dtype=bool)
         self.pending: deque = deque()
@@ -153,24 +164,35 @@ class _Lane:
             # and writes slot 0, which the cold capture pass then recomputes
             self.graphs = {True: self.solver.capture(B, warm=True)} if warm_start else {}
             self.graphs[False] = self.solver.capture(B, warm=False)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
+            self.graphs[False].replay()
+            t1.record()
+        t1.synchronize()
+        self.t_energy = t0.elapsed_time(t1) * 1e-3 / B  # seconds per energy of a full cold batch
         self.buf = self.solver._bufs[B]
 
-    def launch(self, items: list, warm: bool) -> None:
+    def launch(self, items: list, warm: bool, urgent: bool = False) -> None:
         slot = self.free_slots.pop()
         st = self.stage[slot]
         idx = np.array([r.grid_index[p] for r, p in items], dtype=np.int64)
         st["idx"][:idx.size] = torch.from_numpy(idx)
         st["idx"][idx.size:] = int(idx[-1])  # padding repeats the last energy
-        with torch.cuda.stream(self.stream):
+        stream = self.streams[urgent]
+        with torch.cuda.stream(stream):
+            if self.last is not None:
+                stream.wait_event(self.last)
             self.buf["idx"].copy_(st["idx"], non_blocking=True)
             self.graphs[warm].replay()
             st["T"].copy_(self.buf["T"], non_blocking=True)
             st["dens"].copy_(self.buf["density"], non_blocking=True)
             st["cur"].copy_(self.buf["current"], non_blocking=True)
             ev = torch.cuda.Event()
-            ev.record(self.stream)
+            ev.record(stream)
+        self.last = ev
         self.inflight.append((ev, slot, items, idx, warm))
         self.batches["warm" if warm else "cold"] += 1
+        self.urgent_batches += int(urgent)
 
     def poll(self, now: float, done: list) -> None:
         while self.inflight and self.inflight[0][0].query():
@@ -189,11 +211,26 @@ class _Lane:
                 self.cached[idx] = True
             self.free_slots.append(slot)
 
-    def try_launch(self) -> bool:
+    def remaining_cost(self, req: Request) -> float:
+        return req.remaining * self.t_energy
+
+    def try_launch(self, threshold: float = -1.0) -> bool:
+        """Launches the next batch if a staging slot is free. The batch goes
+        to the high-priority stream when its oldest request's remaining work
+        is at most ``threshold`` seconds (shortest remaining work first
+        across lanes)."""
         if not self.free_slots or not self.pending:
             return False
+        if len({r.rid for r, _ in self.pending}) > 1:
+            # shortest remaining work first within the lane as well (stable:
+            # each request's energies keep their order)
+            ordered = sorted(self.pending, key=lambda it: it[0].remaining)
+            self.pending.clear()
+            self.pending.extend(ordered)
+        head = self.pending[0][0]
+        urgent = self.remaining_cost(head) <= threshold
         items, warm = form_batch(self.pending, self.cached, self.B)  # cached stays False without warm starts
-        self.launch(items, warm)
+        self.launch(items, warm, urgent)
         return True
 
 
@@ -222,6 +259,7 @@ class EnergyServer:
                       for k, (j, B) in enumerate(zip(self.catalogue, batches))]
         torch.cuda.synchronize(self.device)
         self.done: list[Request] = []
+        self.active: dict = {}  # rid -> request, submitted and not finished
 
     def submit(self, req: Request, now: float) -> None:
         lane = self.lanes[req.device]
@@ -232,6 +270,7 @@ class EnergyServer:
         req.current = np.zeros((n, N + 1), dtype=np.complex128)
         req.remaining = n
         req.t_submit = now
+        self.active[req.rid] = req
         lane.pending.extend((req, p) for p in range(n))
 
     def pump(self, now: float) -> bool:
@@ -241,8 +280,15 @@ class EnergyServer:
         for lane in self.lanes:
             before = len(self.done)
             lane.poll(now, self.done)
+            for r in self.done[before:]:
+                self.active.pop(r.rid, None)
             busy |= len(self.done) != before
-            while lane.try_launch():
+        # Requests whose remaining work is at or below the median of the
+        # active ones run on the high-priority streams.
+        costs = [self.lanes[r.device].remaining_cost(r) for r in self.active.values()]
+        threshold = float(np.median(costs)) if len(costs) > 1 else -1.0
+        for lane in self.lanes:
+            while lane.try_launch(threshold):
                 busy = True
         return busy
 
@@ -271,7 +317,7 @@ class EnergyServer:
         return {"requests": len(reqs), "energies": energies, "wall_s": wall, "energies_per_s": energies / wall,
                 "warm_fraction": warm / max(energies, 1), "latency": latency_stats([r.latency for r in reqs]),
                 "lanes": [{"device": ln.k, "N": ln.job.num_blocks, "b": ln.job.block_size, "batch": ln.B,
-                           **ln.batches} for ln in self.lanes]}
+                           "urgent": ln.urgent_batches, **ln.batches} for ln in self.lanes]}
 
     def solve_now(self, req: Request) -> Request:
         """Serves one request alone (submit, drain) — the reference point of
