@@ -15,7 +15,7 @@
 // in 16-byte units), and conjugation is a compile-time sign flip.
 //
 // Tiles: CTA 64x64 complex, 4 warps of 32x32, BK = 8 complex per stage,
-// 3-stage cp.async pipeline (zero-filled at the matrix edges). The epilogue
+// 4-stage cp.async pipeline (zero-filled at the matrix edges). The epilogue
 // fuses up to four scaled (optionally conjugate-transposed) addends, a
 // conjugate-transposed second store and a second output with its own
 // addends, so chains like  S = A_jj - Sigma - P A_ij  or
@@ -31,7 +31,7 @@ namespace {
 constexpr int BM = 64;
 constexpr int BN = 64;
 constexpr int BK = 8;
-constexpr int STAGES = 3;
+constexpr int STAGES = 4;
 constexpr int THREADS = 128;
 constexpr int WM = 32;
 constexpr int WN = 32;
