@@ -602,6 +602,26 @@ def run_cfg2(args, local):
         torch.cuda.empty_cache()
     f, m = probe["fp64"], probe["mixed"]
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    # The complex128 oracle (the reference algorithm on the host cores) on one
+    # probe energy: errors of both GPU paths against it.
+    oracle_err = None
+    if not args.no_cpu:
+        from oracle import negf_oracle as o
+
+        k = 1  # probe energy index idx[1]
+        e1 = dev.energies[idx[k:k + 1]]
+        d1, u1, l1 = dev.system_blocks(e1)
+        t0 = time.perf_counter()
+        ref = o.energy_point_solve(d1, u1, l1, dev.fermi_left(e1), dev.fermi_right(e1))
+        osec = time.perf_counter() - t0
+        oxr = np.stack([x[0] for x in ref["xr_diag"]]) if "xr_diag" in ref else None
+        oracle_err = {"energy": float(e1[0]), "oracle_seconds": osec}
+        for name, pr in (("fp64", f), ("mixed", m)):
+            e = {"transmission_rel": float(abs(pr[0][k] - ref["transmission"][0]) / abs(ref["transmission"][0])),
+                 "density_rel": rel(pr[1][k], ref["density"][0])}
+            if oxr is not None:
+                e["g_retarded_diag_rel"] = rel(pr[2][:, k], oxr)
+            oracle_err[name] = e
     fl_e = flops_per_energy(64, 512, (out["mixed"]["sr_iterations"],) * 2)["total"]
     line = {
         "metric": "RGF energy-points/s at 512x512 blocks (mixed)", "value": out["mixed"]["value"],
@@ -617,6 +637,7 @@ def run_cfg2(args, local):
         "error_vs_fp64": {"transmission_max_rel": float(np.max(np.abs(m[0] - f[0]) / np.abs(f[0]))),
                           "density_rel": rel(m[1], f[1]), "g_retarded_diag_rel": rel(m[2], f[2]),
                           "probe": f"energies {idx.tolist()}"},
+        "error_vs_oracle": oracle_err,
     }
     print(json.dumps(line), flush=True)
 
