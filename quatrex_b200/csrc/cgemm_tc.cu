@@ -382,8 +382,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) cgemm_tc_kernel(const Ar
       }
       const bool more = kb + 1 < KB;
       if (more) load_regs<OPA, OPB, VEC>(a, Ag, Bg, R, m0, n0, (kb + 1) * TK, tid);
-      if (!mbar_wait(bar, phase)) ok = false;
+      // One thread polls the MMA-completion barrier; the others wait at the
+      // block barrier instead of spinning on shared memory.
+      if (tid == 0 && !mbar_wait(bar, phase)) ok = false;
       phase ^= 1u;
+      ok = __syncthreads_and(ok);
       if (more && ok) {
         store_planes<OPA, OPB>(R, planes, tid);
         fence_async_smem();
