@@ -17,7 +17,7 @@ import torch
 
 from . import _native
 from ._interop import BTView, default_device, from_device, kind, obc_mats
-from ._native import NULL_MAT, QtxMat
+from ._native import NULL_MAT
 from .utils import get_batches, workspace_pool
 
 

@@ -34,7 +34,7 @@ import torch
 from . import _native
 from ._interop import mat
 from ._native import NULL_MAT, QtxBT, QtxMat
-from .obc import SanchoRubio, fixed_point_refine
+from .obc import SanchoRubio
 from .utils import WorkspacePool
 
 _C128 = torch.complex128
