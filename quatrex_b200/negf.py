@@ -87,6 +87,11 @@ class EnergyPointSolver:
         and runs its products on tcgen05 as split-TF32 products with FP32
         accumulation, inverting every Schur complement in FP64; the
         transmission is formed in FP64 from the complex64 corner block.
+    potential : (N, b) real array, optional
+        Electrostatic potential per orbital, subtracted on the diagonal of
+        A(E) like ``ElectronSolver._assemble_system_matrix``
+        (``electron/solver.py:668-709``, potential at :701); the leads use the
+        potential of their edge blocks.
     store_blocks : bool
         True (default): the G^<, G^> (diagonal and off-diagonal) and G^R
         diagonal blocks of the last batch are kept in ``PointResult.blocks``.
@@ -98,7 +103,8 @@ class EnergyPointSolver:
     def __init__(self, h_diag, coupling, eta: float = 1e-4, sr_tol: float = 1e-12,
                  sr_max_iterations: int = 100, per_energy: bool = True,
                  skip_zero_scattering: bool = False, device: torch.device | None = None,
-                 precision: str = "fp64", device_loop: bool = False, store_blocks: bool = True):
+                 precision: str = "fp64", device_loop: bool = False, store_blocks: bool = True,
+                 potential=None):
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -106,6 +112,13 @@ class EnergyPointSolver:
         h = torch.as_tensor(np.asarray(h_diag), dtype=_C128) if not isinstance(h_diag, torch.Tensor) else h_diag
         t = torch.as_tensor(np.asarray(coupling), dtype=_C128) if not isinstance(coupling, torch.Tensor) else coupling
         self.h = h.to(self.device, _C128).contiguous()
+        if potential is not None:
+            # A_ii = (E + i eta) I - H_ii - diag(V_i): the energy-independent
+            # potential is folded into the resident diagonal blocks once.
+            v = torch.as_tensor(np.asarray(potential, dtype=np.float64)).to(self.device)
+            if v.shape != self.h.shape[:2]:
+                raise ValueError(f"potential must have shape {tuple(self.h.shape[:2])}, got {tuple(v.shape)}")
+            self.h = self.h + torch.diag_embed(v.to(_C128))
         self.N, self.b = int(self.h.shape[0]), int(self.h.shape[-1])
         self.upper = (-t).to(self.device, _C128).contiguous()
         self.lower = (-t.conj().transpose(-2, -1)).to(self.device, _C128).contiguous()

@@ -185,3 +185,22 @@ def test_sr_fixed_point_residual_cfg1(cuda_device):
     s.solve(e, dev.fermi_left(e), dev.fermi_right(e))
     rel, _ = s.last_residuals
     assert float(rel.max()) < 1e-6
+
+
+def test_potential_matches_oracle(cuda_device):
+    """A(E) = (E + i eta) I - H - diag(V) (electron/solver.py:668-709,
+    potential at :701): the potential-shifted device against the oracle on
+    the same shifted blocks."""
+    dev = synthetic.make_device(6, 32, np.linspace(-1.2, 1.2, 6), seed=41)
+    V = np.linspace(0.0, 0.3, dev.num_blocks * dev.block_size).reshape(dev.num_blocks, dev.block_size)
+    s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True, potential=V)
+    r = s.solve(dev.energies, dev.fermi_left(), dev.fermi_right())
+    diag, upper, lower = dev.system_blocks()
+    diag = [d - np.diag(V[i])[None] for i, d in enumerate(diag)]
+    ref = o.energy_point_solve(diag, upper, lower, dev.fermi_left(), dev.fermi_right())
+    t = r.transmission.cpu().numpy()
+    assert np.abs(t - ref["transmission"]).max() / np.abs(ref["transmission"]).max() < TOL_E2E
+    dn = r.density.cpu().numpy()
+    assert np.linalg.norm(dn - ref["density"]) / np.linalg.norm(ref["density"]) < TOL_E2E
+    with pytest.raises(ValueError):
+        EnergyPointSolver(dev.h_diag, dev.coupling, potential=V[:, :3])
