@@ -46,9 +46,9 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--batch", type=int, default=148)
     p.add_argument("--energies", type=int, default=1024)
-    p.add_argument("--e2e-batch", type=int, default=32, help="energies per end-to-end step (host memory: "
-                   "six pinned block-tridiagonal stacks of this many energies)")
-    p.add_argument("--e2e-subbatch", type=int, default=8, help="RGF max_batch_size of the end-to-end leg")
+    p.add_argument("--e2e-batch", type=int, default=64, help="energies per end-to-end step (host memory: "
+                   "six pinned block-tridiagonal stacks of this many energies, ~38 GB at 64)")
+    p.add_argument("--e2e-subbatch", type=int, default=16, help="RGF max_batch_size of the end-to-end leg")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-energies", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
