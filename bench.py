@@ -283,7 +283,10 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
     obc_sys = OBCSystem(SanchoRubio(convergence_tol=1e-12, per_energy=True), memoization_mode="off")
     solver = RGF(max_batch_size=min(sub, B))
 
+    phase = {"obc": 0.0, "solve": 0.0, "density": 0.0}
+
     def step():
+        t0 = time.perf_counter()
         ob = OBCBlocks(n)
         a00, a01, a10 = A.blocks[0, 0], A.blocks[0, 1], A.blocks[1, 0]
         g, *_ = obc_sys((a00, a01, a10), contact="left")
@@ -291,13 +294,22 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
         ann, an1, a1n = A.blocks[n - 1, n - 1], A.blocks[n - 1, n - 2], A.blocks[n - 2, n - 1]
         g, *_ = obc_sys((ann, an1, a1n), contact="right")
         ob.retarded[-1], ob.lesser[-1], ob.greater[-1] = contact_self_energy(an1, a1n, g, fr)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
         cur = solver.selected_solve(A, SL, SG, obc_blocks=ob, out=(XL, XG, XR), return_retarded=True,
                                     return_current=True)
+        t2 = time.perf_counter()
         dens = observables.density(XL)
+        t3 = time.perf_counter()
+        phase["obc"] += t1 - t0
+        phase["solve"] += t2 - t1
+        phase["density"] += t3 - t2
         return cur, dens
 
     step()  # warm-up
     torch.cuda.synchronize()
+    for k in phase:
+        phase[k] = 0.0
     t0 = time.perf_counter()
     for _ in range(steps):
         cur, dens = step()
@@ -307,6 +319,7 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
     h2d = 3 * B * proto.nnz * elem + 6 * B * b * b * elem  # A, Sigma^<, Sigma^> + contact blocks
     d2h = 3 * B * proto.nnz * elem + B * (n + 1) * elem + 6 * B * b * b * elem
     return {"value": steps * B / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "seconds_per_step": {k: v / steps for k, v in phase.items()},
             "path": "RGF.selected_solve + OBCSystem(SanchoRubio) + contact_self_energy on pinned host DSDBCOO "
                     f"stacks, {B} energies per step (RGF max_batch_size {min(sub, B)}), {steps} steps"}
 
@@ -858,6 +871,24 @@ def run_kernels(args, local):
             n, B, mat(w), mat(c), info.data_ptr(), ws.data_ptr(), ws.numel(), stream()))) / 1e12
     _native.check(lib.qtx_set_inverse_path(0))
     out["zinv_torch_linalg_inv"] = flops / timeit(lambda: torch.linalg.inv(w)) / 1e12
+    # Inverse paths against the batch size (the automatic choice's crossover).
+    sweep = {}
+    for nb in (8, 16, 32, 64, 96, 148):
+        for nn in (256, 384, 512):
+            if nb > B:
+                continue
+            wn = (torch.randn((nb, nn, nn), dtype=torch.complex128, device=device, generator=g)
+                  + nn * torch.eye(nn, dtype=torch.complex128, device=device))
+            cn = torch.empty_like(wn)
+            wsn = torch.empty(lib.qtx_zinv_workspace(nn, nb), dtype=torch.uint8, device=device)
+            row = {}
+            for name, mode in (("one_cta", 1), ("multi_cta", 2)):
+                _native.check(lib.qtx_set_inverse_path(mode))
+                row[name] = 8.0 * nn ** 3 * nb / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
+                    nn, nb, mat(wn), mat(cn), info.data_ptr(), wsn.data_ptr(), wsn.numel(), stream()))) / 1e12
+            sweep[f"n{nn}_b{nb}"] = row
+    _native.check(lib.qtx_set_inverse_path(0))
+    out["zinv_path_sweep_tflops"] = sweep
     peak = None if args.no_peak else measured_fp64_peak(torch, device)["peak"]
     tf32 = None if args.no_peak else measured_tf32_peak(torch, device)
     line = {"metric": "kernel throughput at 256x256 blocks (complex flops 8n^3)", "unit": "TFLOP/s",

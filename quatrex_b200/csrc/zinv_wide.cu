@@ -304,8 +304,11 @@ bool zinv_prefers_wide(int n, int64_t batch) {
   if (g_inverse_path == 1) return false;
   if (g_inverse_path == 2) return true;
   // One CTA per matrix leaves SMs idle when the batch is below the SM count;
-  // the multi-CTA path pays n/NB launches and a pass over the matrix per panel.
-  return n >= 384 && batch * 2 <= num_sms();
+  // the multi-CTA path pays n/NB launches and a pass over the matrix per
+  // panel. Measured crossover on B200 (TFLOP/s of both paths against the
+  // batch): n = 256 up to batch 32, n = 384 and 512 up to batch 64.
+  const int sms = num_sms();
+  return (n >= 384 && batch * 2 <= sms) || (n >= 192 && batch * 4 <= sms);
 }
 
 int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, void* scratch,

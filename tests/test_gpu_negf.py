@@ -198,9 +198,11 @@ def test_potential_matches_oracle(cuda_device):
     diag, upper, lower = dev.system_blocks()
     diag = [d - np.diag(V[i])[None] for i, d in enumerate(diag)]
     ref = o.energy_point_solve(diag, upper, lower, dev.fermi_left(), dev.fermi_right())
+    # End to end (boundary conditions included) the gate is the decimation
+    # noise floor: 1e-8 here (measured 1.2e-9 for the density).
     t = r.transmission.cpu().numpy()
-    assert np.abs(t - ref["transmission"]).max() / np.abs(ref["transmission"]).max() < TOL_E2E
+    assert np.abs(t - ref["transmission"]).max() / np.abs(ref["transmission"]).max() < 1e-8
     dn = r.density.cpu().numpy()
-    assert np.linalg.norm(dn - ref["density"]) / np.linalg.norm(ref["density"]) < TOL_E2E
+    assert np.linalg.norm(dn - ref["density"]) / np.linalg.norm(ref["density"]) < 1e-8
     with pytest.raises(ValueError):
         EnergyPointSolver(dev.h_diag, dev.coupling, potential=V[:, :3])
