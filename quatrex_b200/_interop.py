@@ -69,7 +69,15 @@ def from_device(t: torch.Tensor, like):
     """Returns ``t`` as the array type of ``like``."""
     k = kind(like)
     if k == "torch":
-        return t if t.device == like.device else t.to(like.device)
+        if t.device == like.device:
+            return t
+        if like.device.type == "cpu" and t.is_cuda:
+            # pinned host result: the copy is a DMA, and so is a later upload
+            out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            out.copy_(t, non_blocking=True)
+            torch.cuda.current_stream(t.device).synchronize()
+            return out
+        return t.to(like.device)
     if k == "cupy":
         import cupy  # noqa: PLC0415 - only present when the caller uses CuPy
 

@@ -38,8 +38,15 @@ class _BlockIndexer:
         i, j = (i + n) % n, (j + n) % n
         lead = tuple(m.data.shape[:-1])
         bi, bj = int(m.block_sizes[i]), int(m.block_sizes[j])
-        out = torch.zeros(lead + (bi, bj), dtype=m.data.dtype, device=m.data.device)
         e = m._layout.entries.get((i, j)) if abs(i - j) <= 1 else _generic_entry(m, i, j)
+        pin = m.data.device.type == "cpu" and m.data.is_pinned()
+        if e is not None and e.dense:
+            # block-sorted dense block: a fresh copy of its contiguous range
+            # (pinned when the container is, so an upload is a plain DMA)
+            out = torch.empty(lead + (bi, bj), dtype=m.data.dtype, device=m.data.device, pin_memory=pin)
+            out.copy_(m.data[..., e.start:e.stop].reshape(lead + (bi, bj)))
+            return out
+        out = torch.zeros(lead + (bi, bj), dtype=m.data.dtype, device=m.data.device, pin_memory=pin)
         if e is None:
             return out
         r = torch.from_numpy(e.rows.astype(np.int64)).to(m.data.device)
