@@ -17,7 +17,7 @@ import torch
 
 from . import _native
 from ._interop import BTView, default_device, from_device, kind, obc_mats
-from ._native import NULL_MAT
+from ._native import NULL_MAT, QtxMat
 from .utils import get_batches, workspace_pool
 
 
@@ -66,11 +66,20 @@ class RGF(GFSolver):
         the reference (default 100).
     device : torch.device, optional
         CUDA device; defaults to the current device.
+    precision : "fp64" (default) or "mixed"
+        "mixed": ``selected_solve`` runs on complex64 copies of the blocks with
+        split-TF32 tensor-core products and FP64 inverses of the Schur
+        complements (``qtx_selected_solve_mixed``); inputs and outputs keep
+        the containers' complex128 type. ``selected_inv`` is always FP64.
     """
 
-    def __init__(self, max_batch_size: int = 100, device: torch.device | None = None) -> None:
+    def __init__(self, max_batch_size: int = 100, device: torch.device | None = None,
+                 precision: str = "fp64") -> None:
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.max_batch_size = max_batch_size
         self.device = device
+        self.precision = precision
 
     def _dev(self) -> torch.device:
         return self.device if self.device is not None else default_device()
@@ -156,17 +165,11 @@ class RGF(GFSolver):
             batch = A.batch
             cur = torch.zeros((batch, n + 1), dtype=torch.complex128, device=device) if return_current else None
             abi = [v.abi() if v is not None else None for v in (A, SL, SG, XL, XG, XR)]
-            ws_bytes = lib.qtx_selected_solve_workspace(n, abi[0].block_sizes, batch, int(return_current))
-            ws = workspace_pool.get(ws_bytes, device, "rgf")
             info = torch.zeros(batch, dtype=torch.int32, device=device)
             sym = bool(getattr(xl, "symmetry", False)) or bool(getattr(xg, "symmetry", False))
             flags = _native.QTX_SOLVE_SYMMETRIC_OUT if sym else 0
-            _native.check(lib.qtx_selected_solve(
-                ctypes.byref(abi[0]), ctypes.byref(abi[1]), ctypes.byref(abi[2]), orr, ol, og,
-                ctypes.byref(abi[3]), ctypes.byref(abi[4]),
-                ctypes.byref(abi[5]) if abi[5] is not None else None,
-                cur.data_ptr() if cur is not None else None, NULL_MAT, None, flags, batch,
-                info.data_ptr(), ws.data_ptr(), ws.numel(), st))
+            _solve_call(lib, self.precision, abi, (orr, ol, og), cur, info,
+                        lambda nb: workspace_pool.get(nb, device, "rgf"), flags, batch, st, device)
             _raise_if_singular(info)
             XL.finalize(write_lower=not getattr(xl, "symmetry", False))
             XG.finalize(write_lower=not getattr(xg, "symmetry", False))
@@ -228,15 +231,11 @@ class RGF(GFSolver):
             batch = A.batch
             cur = torch.zeros((batch, n + 1), dtype=torch.complex128, device=device) if return_current else None
             abi = [v.abi() if v is not None else None for v in views]
-            ws_bytes = lib.qtx_selected_solve_workspace(n, abi[0].block_sizes, batch, int(return_current))
-            ws = workspace_pool.get(ws_bytes, device, "rgf")
             info = torch.zeros(batch, dtype=torch.int32, device=device)
-            _native.check(lib.qtx_selected_solve(
-                ctypes.byref(abi[0]), ctypes.byref(abi[1]), ctypes.byref(abi[2]), obcs[0], obcs[1], obcs[2],
-                ctypes.byref(abi[3]), ctypes.byref(abi[4]),
-                ctypes.byref(abi[5]) if abi[5] is not None else None,
-                cur.data_ptr() if cur is not None else None, NULL_MAT, None, flags, batch,
-                info.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.c_void_p(comp.cuda_stream)))
+            _solve_call(lib, self.precision, abi, obcs, cur, info,
+                        lambda nb: workspace_pool.get(nb, device, "rgf"), flags, batch,
+                        ctypes.c_void_p(comp.cuda_stream), device)
+            keep.append(abi)
             done = torch.cuda.Event()
             done.record(comp)
             with torch.cuda.stream(down_s):
@@ -272,6 +271,98 @@ class RGF(GFSolver):
         if return_current:
             return current
         return None
+
+
+def _block_shapes(bs, n):
+    return ([(bs[i], bs[i]) for i in range(n)], [(bs[i], bs[i + 1]) for i in range(n - 1)],
+            [(bs[i + 1], bs[i]) for i in range(n - 1)])
+
+
+def _convert(lib, rows, cols, batch, src, src_t, dst, dst_t, stream):
+    _native.check(lib.qtx_convert(rows, cols, batch, src, src_t, dst, dst_t, stream))
+
+
+def _solve_call(lib, precision, abi, obcs, cur, info, ws_getter, flags, batch, stream, device):
+    """One selected-solve call on the given complex128 block views; the mixed
+    precision converts them to complex64 copies, solves, and converts the
+    outputs back into the views."""
+    n = abi[0].num_blocks
+    bs = [int(abi[0].block_sizes[i]) for i in range(n)]
+    if precision == "fp64":
+        ws = ws_getter(lib.qtx_selected_solve_workspace(n, abi[0].block_sizes, batch, int(cur is not None)))
+        _native.check(lib.qtx_selected_solve(
+            ctypes.byref(abi[0]), ctypes.byref(abi[1]), ctypes.byref(abi[2]), obcs[0], obcs[1], obcs[2],
+            ctypes.byref(abi[3]), ctypes.byref(abi[4]), ctypes.byref(abi[5]) if abi[5] is not None else None,
+            cur.data_ptr() if cur is not None else None, NULL_MAT, None, flags, batch,
+            info.data_ptr(), ws.data_ptr(), ws.numel(), stream))
+        return
+    c128, c64 = _native.QTX_C128, _native.QTX_C64
+    keep: list = []
+    shapes = _block_shapes(bs, n)
+
+    def low(bt, role):
+        """complex64 twin of a block-tridiagonal view (inputs converted)."""
+        parts = []
+        for k, arr in enumerate((bt.diag, bt.upper, bt.lower)):
+            cnt = n if k == 0 else n - 1
+            out = []
+            for i in range(max(cnt, 0)):
+                m = arr[i]
+                if not m.ptr:
+                    out.append(NULL_MAT)
+                    continue
+                r, c = shapes[k][i]
+                t = (torch.empty if role == "in" else torch.zeros)((batch, r, c), dtype=torch.complex64,
+                                                                   device=device)
+                keep.append(t)
+                q = QtxMat(t.data_ptr(), c, r * c)
+                if role == "in":
+                    _convert(lib, r, c, batch, m, c128, q, c64, stream)
+                out.append(q)
+            parts.append(out)
+        d = (QtxMat * n)(*parts[0])
+        u = (QtxMat * max(n - 1, 1))(*(parts[1] or [NULL_MAT]))
+        lo = (QtxMat * max(n - 1, 1))(*(parts[2] or [NULL_MAT]))
+        keep.extend([d, u, lo])
+        return _native.QtxBT(n, bt.block_sizes, d, u, lo), parts
+
+    def low_obc(arr):
+        if arr is None:
+            return None
+        out = (QtxMat * n)(*([NULL_MAT] * n))
+        for i in range(n):
+            m = arr[i]
+            if m.ptr:
+                t = torch.empty((batch, bs[i], bs[i]), dtype=torch.complex64, device=device)
+                keep.append(t)
+                q = QtxMat(t.data_ptr(), bs[i], bs[i] * bs[i])
+                _convert(lib, bs[i], bs[i], batch, m, c128, q, c64, stream)
+                out[i] = q
+        keep.append(out)
+        return out
+
+    lo_in = [low(abi[k], "in")[0] for k in range(3)]
+    lo_out = [low(abi[k], "out") if abi[k] is not None else None for k in (3, 4, 5)]
+    lo_obc = [low_obc(o) for o in obcs]
+    ws = ws_getter(lib.qtx_selected_solve_mixed_workspace(n, abi[0].block_sizes, batch, int(cur is not None)))
+    _native.check(lib.qtx_selected_solve_mixed(
+        ctypes.byref(lo_in[0]), ctypes.byref(lo_in[1]), ctypes.byref(lo_in[2]), lo_obc[0], lo_obc[1], lo_obc[2],
+        ctypes.byref(lo_out[0][0]), ctypes.byref(lo_out[1][0]),
+        ctypes.byref(lo_out[2][0]) if lo_out[2] is not None else None,
+        cur.data_ptr() if cur is not None else None, NULL_MAT, None, flags, batch,
+        info.data_ptr(), ws.data_ptr(), ws.numel(), stream))
+    symmetric = bool(flags & _native.QTX_SOLVE_SYMMETRIC_OUT)
+    for k, lo in zip((3, 4, 5), lo_out):
+        if lo is None:
+            continue
+        bt, parts = abi[k], lo[1]
+        for kk, arr in enumerate((bt.diag, bt.upper, bt.lower)):
+            if kk == 2 and symmetric:
+                continue  # not written by the solve: the container keeps its values
+            for i, q in enumerate(parts[kk]):
+                if q.ptr and arr[i].ptr:
+                    r, c = shapes[kk][i]
+                    _convert(lib, r, c, batch, q, c64, arr[i], c128, stream)
 
 
 def _on_host(m) -> bool:

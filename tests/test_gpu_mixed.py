@@ -89,3 +89,41 @@ def test_mixed_energy_point_errors_vs_fp64(cfg0_pair):
     }
     print("mixed vs fp64 (cfg0):", errs)
     assert errs["transmission"] < 1e-3 and errs["density"] < 1e-3 and errs["xr_diag"] < 1e-3, errs
+
+
+@pytest.mark.parametrize("symmetric", [False, True])
+def test_rgf_plugin_mixed_precision(cuda_device, symmetric):
+    """RGF(precision="mixed") through the qttools-style interface: complex128
+    containers in and out, split-TF32 solve inside; within the mixed path's
+    stated accuracy of the FP64 plugin path on a well-conditioned system."""
+    import scipy.sparse as sps
+
+    from quatrex_b200 import RGF, DSDBCOO, synthetic
+
+    bs = np.array([8, 16, 12, 16])
+    dense = synthetic.random_bt_dense(bs, seed=5) + 4.0 * np.eye(bs.sum())
+    bl = sps.coo_matrix(dense)
+    bl = sps.coo_matrix(bl - bl.conj().T)
+    bg = sps.coo_matrix(1j * dense)
+    bg = sps.coo_matrix(bg - bg.conj().T)
+
+    def dev(m):
+        x = DSDBCOO.from_sparray(m, bs, (6,))
+        return DSDBCOO(x.data.to(cuda_device), x.rows, x.cols, x.block_sizes, x.global_stack_shape)
+
+    out = {}
+    for prec in ("fp64", "mixed"):
+        A, Bl, Bg = dev(sps.coo_matrix(dense)), dev(bl), dev(bg)
+        Xl, Xg, Xr = (DSDBCOO.zeros_like(A) for _ in range(3))
+        for X in (Xl, Xg):
+            X.data.fill_(5.0 + 1.0j)
+            X.symmetry = symmetric
+        cur = RGF(max_batch_size=4, precision=prec).selected_solve(A, Bl, Bg, out=(Xl, Xg, Xr),
+                                                                   return_retarded=True, return_current=True)
+        out[prec] = [X.data.cpu().numpy() for X in (Xl, Xg, Xr)] + [cur.cpu().numpy()]
+    for a, b in zip(out["mixed"], out["fp64"]):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
+    if symmetric:  # lower blocks untouched in both paths
+        np.testing.assert_array_equal(out["mixed"][0] == 5.0 + 1.0j, out["fp64"][0] == 5.0 + 1.0j)
+    with pytest.raises(ValueError):
+        RGF(precision="half")
