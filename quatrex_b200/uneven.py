@@ -313,9 +313,11 @@ class UnevenBatchRunner:
             self.states.append(st)
         torch.cuda.synchronize(dev)
 
-    def enqueue(self) -> None:
+    def enqueue(self, nested: bool = True) -> None:
         """Enqueues every batch of every job, round-robin over the jobs, each
-        job on its own stream. Returns without synchronising."""
+        job on its own stream. Returns without synchronising. ``nested=False``
+        issues the pipelines' kernels instead of replaying the per-device
+        graphs (used while capturing the whole schedule)."""
         cur = torch.cuda.current_stream(self.device)
         for st in self.states:
             st.stream.wait_stream(cur)
@@ -329,7 +331,10 @@ class UnevenBatchRunner:
                 with torch.cuda.stream(st.stream):
                     st.solver.set_inputs_device(st.energies[lo:lo + B], st.f_left[lo:lo + B],
                                                 st.f_right[lo:lo + B])
-                    st.graph.replay()
+                    if nested:
+                        st.graph.replay()
+                    else:
+                        st.solver._run(B, device_loop=True)
                     res = st.solver._result(B)
                     n = hi - lo
                     st.transmission[lo:hi].copy_(res.transmission[:n], non_blocking=True)
@@ -337,6 +342,25 @@ class UnevenBatchRunner:
                     st.current[lo:hi].copy_(res.current[:n], non_blocking=True)
         for st in self.states:
             cur.wait_stream(st.stream)
+
+    def capture_all(self) -> "torch.cuda.CUDAGraph":
+        """The whole schedule of ``enqueue`` — every batch of every device on
+        its own stream, with the input and output copies — captured as one
+        CUDA graph, so that one launch solves the uneven batch. The
+        pipelines' kernels are captured directly (a graph launch inside a
+        capture is not accepted by the runtime here), in the same order as
+        the per-device replays."""
+        if not self.states:
+            self.prepare()
+        dev = self.device
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        torch.cuda.synchronize(dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self.enqueue(nested=False)
+        self.all_graph = g
+        return g
 
     def run(self) -> dict:
         """prepare() if needed, enqueue(), synchronise; returns per-job
