@@ -319,6 +319,7 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
     h2d = 3 * B * proto.nnz * elem + 6 * B * b * b * elem  # A, Sigma^<, Sigma^> + contact blocks
     d2h = 3 * B * proto.nnz * elem + B * (n + 1) * elem + 6 * B * b * b * elem
     return {"value": steps * B / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "energies": steps * B, "seconds": dt,
             "seconds_per_step": {k: v / steps for k, v in phase.items()},
             "path": "RGF.selected_solve + OBCSystem(SanchoRubio) + contact_self_energy on pinned host DSDBCOO "
                     f"stacks, {B} energies per step (RGF max_batch_size {min(sub, B)}), {steps} steps"}
@@ -472,12 +473,27 @@ def run_ours(args, world, rank, local):
 
     e2e = None
     cpu = None
-    if rank == 0 and world == 1:
-        if not args.no_e2e:
-            e2e = e2e_leg(torch, device, dev, dev.energies[np.linspace(0, args.energies - 1, args.e2e_batch)
-                                                               .astype(int)], args.e2e_steps, args.e2e_subbatch)
-        if not args.no_cpu:
-            cpu = cpu_baseline(args.cpu_energies)
+    if not args.no_e2e:
+        # Every rank runs the plugin path on its own energy shard; the batch
+        # per rank shrinks with N so that the pinned host stacks of all ranks
+        # stay near those of one rank at N = 1 (~38 GB).
+        nb = args.e2e_batch if world == 1 else max(8, args.e2e_batch // world)
+        pick = mine[np.linspace(0, mine.size - 1, min(nb, mine.size)).astype(int)]
+        if world > 1:
+            dist.barrier()
+        e2e = e2e_leg(torch, device, dev, dev.energies[pick], args.e2e_steps, min(args.e2e_subbatch, pick.size))
+        if world > 1:
+            agg = torch.tensor([e2e["energies"], e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"]],
+                               dtype=torch.float64, device=device)
+            dist.all_reduce(agg)
+            tmax = torch.tensor([e2e["seconds"]], dtype=torch.float64, device=device)
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            e2e["value"] = float(agg[0].item()) / float(tmax.item())
+            e2e["h2d_bytes_per_step"] = int(agg[1].item())
+            e2e["d2h_bytes_per_step"] = int(agg[2].item())
+            e2e["path"] += f"; {world} ranks, {pick.size} energies per rank, max time over ranks"
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.cpu_energies)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
