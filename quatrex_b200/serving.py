@@ -122,6 +122,16 @@ def slowdown_stats(mixed: dict, alone: dict) -> dict:
             "max": float(r.max())}
 
 
+def order_pending(pending: deque) -> None:
+    """Shortest remaining work first: reorders the (request, position) items
+    by their request's remaining energies, in place. Stable, so each
+    request's energies keep their order and equal requests keep FIFO order."""
+    if len({r.rid for r, _ in pending}) > 1:
+        ordered = sorted(pending, key=lambda it: it[0].remaining)
+        pending.clear()
+        pending.extend(ordered)
+
+
 def latency_stats(latencies) -> dict:
     lat = np.asarray(latencies, dtype=np.float64)
     if lat.size == 0:
@@ -221,12 +231,7 @@ class _Lane:
         across lanes)."""
         if not self.free_slots or not self.pending:
             return False
-        if len({r.rid for r, _ in self.pending}) > 1:
-            # shortest remaining work first within the lane as well (stable:
-            # each request's energies keep their order)
-            ordered = sorted(self.pending, key=lambda it: it[0].remaining)
-            self.pending.clear()
-            self.pending.extend(ordered)
+        order_pending(self.pending)
         head = self.pending[0][0]
         urgent = self.remaining_cost(head) <= threshold
         items, warm = form_batch(self.pending, self.cached, self.B)  # cached stays False without warm starts

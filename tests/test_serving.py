@@ -6,7 +6,7 @@ from collections import deque
 
 import numpy as np
 
-from quatrex_b200.serving import Request, form_batch, latency_stats, poisson_requests
+from quatrex_b200.serving import Request, form_batch, latency_stats, order_pending, poisson_requests, slowdown_stats
 
 
 def test_poisson_workload_is_seeded_and_bounded():
@@ -52,3 +52,23 @@ def test_latency_stats():
     s = latency_stats(np.arange(1, 101, dtype=float))
     assert s["count"] == 100 and abs(s["p50_s"] - 50.5) < 1e-12 and abs(s["p99_s"] - 99.01) < 1e-9
     assert latency_stats([]) == {"count": 0}
+
+
+def test_order_pending_shortest_remaining_first():
+    big = Request(0, 0, np.arange(6))
+    small = Request(1, 0, np.arange(2))
+    mid = Request(2, 0, np.arange(4))
+    big.remaining, small.remaining, mid.remaining = 6, 2, 4
+    pending = deque([(big, p) for p in range(6)] + [(mid, p) for p in range(4)] + [(small, p) for p in range(2)])
+    order_pending(pending)
+    assert [(r.rid, p) for r, p in pending][:6] == [(1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (2, 3)]
+    assert [r.rid for r, _ in pending][6:] == [0] * 6
+    single = deque([(big, 3), (big, 1)])
+    order_pending(single)  # one request: order untouched
+    assert [p for _, p in single] == [3, 1]
+
+
+def test_slowdown_stats():
+    s = slowdown_stats({1: 2.0, 2: 3.0, 3: 1.0}, {1: 1.0, 2: 1.0, 3: 2.0})
+    assert s["count"] == 3 and s["max"] == 3.0 and abs(s["p50"] - 2.0) < 1e-12
+    assert slowdown_stats({}, {}) == {"count": 0}
