@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS peak measurements")
     p.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
                    help="fp64 is the headline value; mixed is reported beside it")
+    p.add_argument("--emulated-slices", type=int, default=6,
+                   help="cfg1 with --precision both: also time the FP64 path with its complex128 products "
+                        "emulated on the int8 tensor cores from this many digit planes (0: skip)")
     p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels"], default="cfg1",
                    help="cfg1 (default): the headline line. cfg2: 64 blocks of 512x512, mixed vs FP64. "
                         "cfg3: eight uneven devices on one GPU. cfg4: the serving loop.")
@@ -155,6 +158,26 @@ def measured_tf32_peak(torch, device) -> float:
         e.synchronize()
         best = min(best, s.elapsed_time(e))
     torch.backends.cuda.matmul.allow_tf32 = old
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_int8_peak(torch, device) -> float:
+    """cuBLASLt int8 GEMM (int32 accumulation), 8192^3, best of 5 (TOPS)."""
+    n = 8192
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device)
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device).t().contiguous().t()
+    torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
     del a, b
     torch.cuda.empty_cache()
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
@@ -348,6 +371,8 @@ def run_ours(args, world, rank, local):
     lib = _native.load()
     peak = {"peak": None} if args.no_peak else measured_fp64_peak(torch, device)
     tf32_peak = None if (args.no_peak or args.precision == "fp64") else measured_tf32_peak(torch, device)
+    emulate = args.precision == "both" and args.emulated_slices > 0
+    int8_peak = measured_int8_peak(torch, device) if (emulate and not args.no_peak) else None
     props = torch.cuda.get_device_properties(device)
     gpu_id = str(getattr(props, "uuid", local))
     if gpu_id and not gpu_id.startswith("GPU-") and len(gpu_id) > 8:
@@ -355,7 +380,8 @@ def run_ours(args, world, rank, local):
 
     def timed(precision):
         solver = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True,
-                                   device=device, precision=precision, device_loop=args.graph)
+                                   device=device, precision=precision, device_loop=args.graph,
+                                   slices=args.emulated_slices if precision == "emulated" else 6)
 
         def step(k):
             idx = batches[k % len(batches)]
@@ -421,7 +447,8 @@ def run_ours(args, world, rank, local):
         return ms, prof, clk, sr_iters, probe_out, per_step, prof_ref_ms
 
     res = {}
-    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]) + (["emulated"] if emulate
+                                                                                         else []):
         res[prec] = timed(prec)
     main_prec = "fp64" if "fp64" in res else "mixed"
     ms, prof, clk, sr_iters, _, per_step, pms = res[main_prec]
@@ -469,6 +496,43 @@ def run_ours(args, world, rank, local):
                               "probe": f"{batches[0].size} energies of the grid"},
             "gpu_launches": mprof["all"][2] * (args.steps if args.graph else 1), "clocks": mclk,
             "latency_ms": _latency(mper, B),
+        }
+
+    emulated_line = None
+    if "emulated" in res and main_prec == "fp64":
+        ems, eprof, eclk, _, eprobe, eper, epms = res["emulated"]
+        te = torch.tensor([ems], dtype=torch.float64, device=device)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        S = args.emulated_slices
+        pairs = S * (S + 1) // 2
+        eg_ms, eg_work, eg_n = eprof["zgemm_emu"]
+        sp_ms, sp_bytes, sp_n = eprof["split"]
+        int8_tops = eg_work * pairs / (eg_ms * 1e-3) / 1e12 if eg_n else None
+        fprobe = res["fp64"][4]
+        terr = np.abs(eprobe[0] - fprobe[0]) / np.abs(fprobe[0])
+        emulated_line = {
+            "value": float(total.item()) / (float(te.item()) * 1e-3), "unit": UNIT,
+            "ms_per_step": float(te.item()) / args.steps,
+            "speedup_vs_fp64": ms_max / float(te.item()),
+            "dtype": f"c128 storage; complex128 products from {S} int8 digit planes per operand "
+                     "(tcgen05 kind::i8, exact int32 sums, FP64 combination); FP64 inverses",
+            "slices": S,
+            "roofline": {"bound": "tensor", "kernel": "oz_gemm_kernel (tcgen05 kind::i8, M=128, N<=256)",
+                         "achieved": int8_tops, "peak": int8_peak, "unit": "int8 TOPS (2 x int8 MACs)",
+                         "frac": (int8_tops / int8_peak) if (int8_tops and int8_peak) else None,
+                         "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
+                         "launches": eg_n, "avg_launch_ms": eg_ms / eg_n if eg_n else None,
+                         "share_of_step_time": eg_ms / epms if epms else None,
+                         "split_share_of_step_time": sp_ms / epms if epms else None,
+                         "class_shares": {k: round(v[0] / epms, 4) for k, v in eprof.items()
+                                          if k != "all" and epms}},
+            "error_vs_fp64": {"transmission_max_rel": float(terr.max()),
+                              "transmission_median_rel": float(np.median(terr)),
+                              "density_rel": float(np.linalg.norm(eprobe[1] - fprobe[1]) / np.linalg.norm(fprobe[1])),
+                              "probe": f"{batches[0].size} energies of the grid"},
+            "gpu_launches": eprof["all"][2] * (args.steps if args.graph else 1), "clocks": eclk,
+            "latency_ms": _latency(eper, B),
         }
 
     e2e = None
@@ -543,6 +607,7 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "latency_ms": _latency(per_step, B),
         "mixed": mixed_line,
+        "emulated": emulated_line,
     }
     print(json.dumps(line), flush=True)
 
@@ -609,10 +674,12 @@ def run_cfg2(args, local):
     job = jobs_from_devices([dev])[0]
     fl, fr = dev.fermi_left(), dev.fermi_right()
     out = {}
-    for prec in ("mixed", "fp64"):
+    emu = ("emulated",) if args.emulated_slices > 0 else ()
+    for prec in ("mixed", "fp64") + emu:
         B = plan_batches([job], args.budget_gb * 1e9, prec)[0]
         s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True, device=device,
-                              precision=prec, device_loop=True, store_blocks=False)
+                              precision=prec, device_loop=True, store_blocks=False,
+                              slices=max(args.emulated_slices, 3))
         sec, clk = _timed_batches(torch, s, dev.energies, fl, fr, B, args.steps, min(args.warmup, 1))
         it = s.sr_status(B)[0]
         out[prec] = {"value": args.steps * B / sec, "batch": B, "seconds": sec, "clocks": clk, "sr_iterations": it}
@@ -621,9 +688,9 @@ def run_cfg2(args, local):
     # Error probe: 4 energies with all blocks kept, both precisions.
     idx = np.linspace(0, ne - 1, 4).astype(int)
     probe = {}
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed") + emu:
         s = EnergyPointSolver(dev.h_diag, dev.coupling, eta=dev.eta, sr_tol=1e-12, per_energy=True, device=device,
-                              precision=prec)
+                              precision=prec, slices=max(args.emulated_slices, 3))
         r = s.solve(dev.energies[idx], fl[idx], fr[idx])
         probe[prec] = (r.transmission.cpu().numpy().copy(), r.density.cpu().numpy().copy(),
                        r.blocks["xr_diag"].to(torch.complex128).cpu().numpy())
@@ -645,7 +712,7 @@ def run_cfg2(args, local):
         osec = time.perf_counter() - t0
         oxr = np.stack([x[0] for x in ref["xr_diag"]]) if "xr_diag" in ref else None
         oracle_err = {"energy": float(e1[0]), "oracle_seconds": osec}
-        for name, pr in (("fp64", f), ("mixed", m)):
+        for name, pr in [("fp64", f), ("mixed", m)] + [(e, probe[e]) for e in emu]:
             e = {"transmission_rel": float(abs(pr[0][k] - ref["transmission"][0]) / abs(ref["transmission"][0])),
                  "density_rel": rel(pr[1][k], ref["density"][0])}
             if oxr is not None:
@@ -668,6 +735,12 @@ def run_cfg2(args, local):
                           "probe": f"energies {idx.tolist()}"},
         "error_vs_oracle": oracle_err,
     }
+    if emu:
+        em = probe["emulated"]
+        line["emulated"] = dict(out["emulated"], slices=args.emulated_slices,
+                                speedup_vs_fp64=out["emulated"]["value"] / out["fp64"]["value"],
+                                error_vs_fp64={"transmission_max_rel": float(np.max(np.abs(em[0] - f[0]) / np.abs(f[0]))),
+                                               "density_rel": rel(em[1], f[1]), "g_retarded_diag_rel": rel(em[2], f[2])})
     print(json.dumps(line), flush=True)
 
 

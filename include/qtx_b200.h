@@ -27,8 +27,9 @@
  *  - Scratch memory is supplied by the caller (workspace pointer + size);
  *    the *_workspace_size functions give the required size in bytes.
  *  - Calls on different streams with disjoint buffers and workspaces are
- *    independent; the library keeps no global mutable state besides the
- *    thread-local error string.
+ *    independent; the library's mutable state is the thread-local error
+ *    string, the thread-local GEMM path (qtx_set_gemm_path), the inverse
+ *    path knob and the launch profiler.
  */
 #ifndef QTX_B200_H
 #define QTX_B200_H
@@ -99,6 +100,33 @@ int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, doubl
 int qtx_cgemm_batched(int m, int n, int k, int64_t batch, float alpha_re, float alpha_im, qtx_mat a,
                       int op_a, qtx_mat b, int op_b, float beta_re, float beta_im, qtx_mat d,
                       int op_d, qtx_mat c, int* err, qtx_stream stream);
+
+/* Batched complex128 GEMM emulated on the int8 tcgen05 tensor cores,
+ * C = alpha op(A) op(B) + beta op(D) as qtx_zgemm_batched. Each operand is
+ * split into `slices` (3-8) int8 planes of balanced base-256 digits under a
+ * power-of-two scale per row of op(A) / column of op(B); digit pairs are
+ * multiplied exactly (int32 tensor-core sums) and combined in FP64
+ * (Ozaki-style splitting). Error per element below
+ * 2 slices k 2^(4 - 8 slices) max_l|op(A)_il| max_l|op(B)_lj|: ~1e-12 relative
+ * at 6 slices, FP64 level at 7. Requires slices * 2k * 2^14 < 2^31.
+ * workspace: qtx_zgemm_emulated_workspace bytes for the whole batch; less
+ * processes the batch in chunks (too little for one entry is an error).
+ * No reference counterpart: a faster evaluation of the same products. */
+size_t qtx_zgemm_emulated_workspace(int m, int n, int k, int64_t batch, int slices);
+int qtx_zgemm_emulated_batched(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                               qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re,
+                               double beta_im, qtx_mat d, int op_d, qtx_mat c, int slices,
+                               void* workspace, size_t workspace_bytes, qtx_stream stream);
+/* GEMM path of the CALLING THREAD for the complex128 drivers (selected
+ * inversion, selected solve, Sancho-Rubio, OBC refinement, contact
+ * self-energy): 0 = FP64 DMMA (default), 3-8 = the int8 emulation with that
+ * many slices. With the emulated path the drivers' *_workspace functions
+ * include its scratch: query them after selecting the path. */
+int qtx_set_gemm_path(int slices);
+int qtx_get_gemm_path(void);
+/* 1 if a bounded wait inside an emulated GEMM timed out since the last call
+ * (the flag is cleared), 0 if not, < 0 on error. Synchronises the device. */
+int qtx_emulated_gemm_status(void);
 
 /* Batched complex128 inverse X = A^{-1} (Gauss-Jordan, partial pivoting).
  * Replaces qttools/kernels/linalg/inv.py:6-40 (numpy.linalg.inv /
@@ -301,7 +329,9 @@ enum qtx_kernel_class {
   QTX_KERNEL_BLOCKOPS = 2, /* elementwise block kernels; work = bytes */
   QTX_KERNEL_REDUCE = 3,   /* traces / norms; work = bytes */
   QTX_KERNEL_FORMAT = 4,   /* assembly, densify / sparsify; work = bytes */
-  QTX_KERNEL_CGEMM = 5     /* complex64 tcgen05 GEMM (split TF32); work = 8 m n k flops */
+  QTX_KERNEL_CGEMM = 5,    /* complex64 tcgen05 GEMM (split TF32); work = 8 m n k flops */
+  QTX_KERNEL_ZGEMM_EMU = 6, /* complex128 GEMM on int8 tcgen05 (digit planes); work = 8 m n k */
+  QTX_KERNEL_SPLIT = 7      /* digit-plane split of the emulated GEMM's operands; work = bytes */
 };
 /* Turns event bracketing of every library kernel launch on or off. */
 int qtx_profile_enable(int on);

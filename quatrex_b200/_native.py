@@ -24,7 +24,8 @@ QTX_SOLVE_SYMMETRIC_OUT = 1
 QTX_C128 = 0
 QTX_C64 = 1
 
-KERNEL_CLASSES = {"zgemm": 0, "zinv": 1, "blockops": 2, "reduce": 3, "format": 4, "cgemm": 5}
+KERNEL_CLASSES = {"zgemm": 0, "zinv": 1, "blockops": 2, "reduce": 3, "format": 4, "cgemm": 5,
+                  "zgemm_emu": 6, "split": 7}
 
 
 class QtxMat(Structure):
@@ -56,6 +57,13 @@ SIGNATURES = {
     "qtx_zinv_workspace": (c_size_t, [c_int, c_int64]),
     "qtx_zinv_batched_ws": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p, c_size_t, c_void_p]),
     "qtx_set_inverse_path": (c_int, [c_int]),
+    "qtx_zgemm_emulated_workspace": (c_size_t, [c_int, c_int, c_int, c_int64, c_int]),
+    "qtx_zgemm_emulated_batched": (c_int, [c_int, c_int, c_int, c_int64, c_double, c_double, QtxMat, c_int,
+                                           QtxMat, c_int, c_double, c_double, QtxMat, c_int, QtxMat, c_int,
+                                           c_void_p, c_size_t, c_void_p]),
+    "qtx_set_gemm_path": (c_int, [c_int]),
+    "qtx_get_gemm_path": (c_int, []),
+    "qtx_emulated_gemm_status": (c_int, []),
     "qtx_selected_inv_workspace": (c_size_t, [c_int32, POINTER(c_int32), c_int64]),
     "qtx_selected_inv": (c_int, [POINTER(QtxBT), POINTER(QtxMat), POINTER(QtxBT), c_int64, c_void_p,
                                  c_void_p, c_size_t, c_void_p]),

@@ -137,6 +137,7 @@ size_t inv_ws_bytes(int32_t nb, const int32_t* bs, int64_t batch) {
   for (int i = 0; i < nb; ++i) ws.mat(bs[i], bs[i], batch);
   for (int k = 0; k < 6; ++k) ws.mat(bm, bm, batch);
   ws.take(zinv_scratch_bytes(bm, batch));
+  ws.take(oz_scratch_bytes(bm, bm, bm, batch, gemm_slices()));
   return ws.off + 256;
 }
 
@@ -233,6 +234,64 @@ int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, v
     return zinv_ex(n, batch, from_abi(a), from_abi(x), info, nullptr, workspace, workspace_bytes,
                    (cudaStream_t)stream);
   });
+}
+
+size_t qtx_zgemm_emulated_workspace(int m, int n, int k, int64_t batch, int slices) {
+  if (m <= 0 || n <= 0 || k <= 0 || batch <= 0 || !oz_supported(k, slices)) return 0;
+  return oz_scratch_bytes(m, n, k, batch, slices) + 256;
+}
+
+int qtx_zgemm_emulated_batched(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                               qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re,
+                               double beta_im, qtx_mat d, int op_d, qtx_mat c, int slices,
+                               void* workspace, size_t workspace_bytes, qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || k < 0 || batch < 0 || (op_a != 0 && op_a != 1) ||
+        (op_b != 0 && op_b != 1) || (op_d != 0 && op_d != 1) || c.ptr == nullptr ||
+        (k > 0 && (a.ptr == nullptr || b.ptr == nullptr))) {
+      set_error("qtx_zgemm_emulated_batched: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    if (!oz_supported(k, slices)) {
+      set_error("qtx_zgemm_emulated_batched: slices must be 3-8 and slices * 2k * 2^14 < 2^31");
+      return (int)QTX_ERR_ARG;
+    }
+    if (m == 0 || n == 0 || batch == 0) return (int)QTX_OK;
+    GemmDesc g;
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.batch = batch;
+    g.A = from_abi(a);
+    g.B = from_abi(b);
+    g.opA = op_a;
+    g.opB = op_b;
+    g.alpha = make_double2(alpha_re, alpha_im);
+    g.C = from_abi(c);
+    if (d.ptr != nullptr) {
+      g.add[0] = Addend{from_abi(d), make_double2(beta_re, beta_im), op_d};
+      g.nadd = 1;
+    }
+    if (k == 0) return zgemm(g, (cudaStream_t)stream);
+    return zgemm_oz(g, slices, workspace, workspace_bytes, (cudaStream_t)stream);
+  });
+}
+
+int qtx_set_gemm_path(int slices) {
+  if (slices != 0 && (slices < 3 || slices > 8)) {
+    set_error("qtx_set_gemm_path: slices must be 0 (FP64 DMMA) or 3-8 (int8 emulation)");
+    return QTX_ERR_ARG;
+  }
+  set_gemm_slices(slices);
+  return QTX_OK;
+}
+
+int qtx_get_gemm_path(void) { return gemm_slices(); }
+
+int qtx_emulated_gemm_status(void) {
+  int flag = 0;
+  const int st = oz_status_take(&flag);
+  return st != QTX_OK ? st : flag;
 }
 
 int qtx_set_inverse_path(int mode) {

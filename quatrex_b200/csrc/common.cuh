@@ -110,6 +110,20 @@ struct GemmDesc {
 
 int zgemm(const GemmDesc& d, cudaStream_t s);
 
+// The same GEMM emulated on the int8 tensor cores with `slices` digit planes
+// per operand (zgemm_oz.cu); `scratch` holds the planes of a batch chunk.
+size_t oz_scratch_bytes(int M, int N, int K, int64_t batch, int slices);
+bool oz_supported(int K, int slices);
+int zgemm_oz(const GemmDesc& d, int slices, void* scratch, size_t bytes, cudaStream_t s);
+// GEMM path of the calling thread: 0 = FP64 DMMA, 3-8 = int8 emulation with
+// that many slices (used where a driver bound scratch for it).
+void set_gemm_slices(int slices);
+int gemm_slices();
+void oz_bind(void* scratch, size_t bytes);
+void* oz_bound(size_t* bytes);
+// Reads and clears the device flag of timed-out waits in the emulated GEMM.
+int oz_status_take(int* flag);
+
 // Complex64 GEMM on tcgen05 with split-TF32 products (cgemm_tc.cu):
 //   C = alpha op(A) op(B) + sum_t coef_t op_t(D_t);  C2 = coef2 C^H (optional).
 struct CAddend {
@@ -222,6 +236,18 @@ struct Workspace {
     m.stride = stride;
     return m;
   }
+};
+
+// Reserves the emulated-GEMM scratch for n x n x n products over `batch`
+// from a driver's workspace when the calling thread selected the int8 path,
+// and binds it to the thread for the scope (restoring the previous binding).
+struct OzScope {
+  OzScope(Workspace& ws, int n, int64_t batch);
+  ~OzScope();
+  OzScope(const OzScope&) = delete;
+  OzScope& operator=(const OzScope&) = delete;
+  void* prev_p;
+  size_t prev_bytes;
 };
 
 // A temporary reshaped to rows x cols inside a larger slot.

@@ -109,6 +109,7 @@ int selected_inv_run(const BTRef& a, const MatRef* obc_r, const BTRef& x, int64_
   MatRef tG[2] = {ws.mat(bm, bm, batch), ws.mat(bm, bm, batch)};
   const size_t scr_bytes = zinv_scratch_bytes(bm, batch);
   void* scr = ws.take(scr_bytes);
+  OzScope oz(ws, bm, batch);
   if (ws.base == nullptr) return QTX_OK;
   if (ws.overflow) {
     set_error("selected_inv: workspace too small");
@@ -294,6 +295,7 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
   MatRef inv_tmp = Prec::kInvTmp ? ws.mat(bm, bm, batch, sizeof(z64)) : MatRef{};
   const size_t inv_scr_bytes = zinv_scratch_bytes(bm, batch);
   void* inv_scr = ws.take(inv_scr_bytes);
+  OzScope oz(ws, Prec::E == sizeof(z64) ? bm : 0, batch);  // complex128 products only
   if (ws.base == nullptr) return QTX_OK;
   if (ws.overflow) {
     set_error("selected_solve: workspace too small");

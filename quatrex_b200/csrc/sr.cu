@@ -107,6 +107,7 @@ size_t sancho_rubio_ws(int n, int64_t batch) {
   ws.take(sizeof(double) * batch);
   ws.take(sizeof(int) * batch);
   ws.take(zinv_scratch_bytes(n, batch));
+  ws.take(oz_scratch_bytes(n, n, n, batch, gemm_slices()));
   return ws.off + 256;
 }
 
@@ -324,6 +325,7 @@ int sancho_rubio_multi_async_run(int n, int nsys, const int64_t* batches, const 
   int64_t total = 0;
   for (int k = 0; k < nsys; ++k) total += batches[k];
   SRState st = sr_state(n, total, ws);
+  OzScope oz(ws, n, total);
   if (ws.overflow) {
     set_error("sancho_rubio_multi_async: workspace too small");
     return QTX_ERR_WORKSPACE;
@@ -347,6 +349,7 @@ int sancho_rubio_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, M
                      int max_iterations, double tol, int per_energy, int* iterations,
                      int* converged, double* delta_out, int* info, Workspace& ws, cudaStream_t s) {
   SRState st = sr_state(n, batch, ws);
+  OzScope oz(ws, n, batch);
   if (ws.overflow) {
     set_error("sancho_rubio: workspace too small");
     return QTX_ERR_WORKSPACE;
@@ -367,6 +370,7 @@ int sancho_rubio_multi_run(int n, int nsys, const int64_t* batches, const qtx_ma
   int64_t total = 0;
   for (int k = 0; k < nsys; ++k) total += batches[k];
   SRState st = sr_state(n, total, ws);
+  OzScope oz(ws, n, total);
   if (ws.overflow) {
     set_error("sancho_rubio_multi: workspace too small");
     return QTX_ERR_WORKSPACE;
@@ -390,6 +394,7 @@ size_t obc_refine_ws(int n, int64_t batch) {
   Workspace ws;
   for (int k = 0; k < 2; ++k) ws.mat(n, n, batch);
   ws.take(zinv_scratch_bytes(n, batch));
+  ws.take(oz_scratch_bytes(n, n, n, batch, gemm_slices()));
   return ws.off + 256;
 }
 
@@ -398,6 +403,7 @@ int obc_refine_run(int n, int64_t batch, MatRef aii, MatRef aij, MatRef aji, Mat
   MatRef T = ws.mat(n, n, batch), S = ws.mat(n, n, batch);
   const size_t scr_bytes = zinv_scratch_bytes(n, batch);
   void* scr = ws.take(scr_bytes);
+  OzScope oz(ws, n, batch);
   if (ws.overflow) {
     set_error("obc_refine: workspace too small");
     return QTX_ERR_WORKSPACE;
@@ -415,6 +421,7 @@ size_t contact_ws(int n, int64_t batch) {
   Workspace ws;
   ws.mat(n, n, batch);
   ws.mat(n, n, batch);
+  ws.take(oz_scratch_bytes(n, n, n, batch, gemm_slices()));
   return ws.off + 256;
 }
 
@@ -422,6 +429,7 @@ int contact_run(int n, int64_t batch, MatRef aij, MatRef aji, MatRef g, const do
                 MatRef sigma, MatRef sl, MatRef sg, Workspace& ws, cudaStream_t s) {
   MatRef T = ws.mat(n, n, batch);
   MatRef Sg = sigma.null() ? ws.mat(n, n, batch) : sigma;
+  OzScope oz(ws, n, batch);
   if (ws.overflow) {
     set_error("contact_self_energy: workspace too small");
     return QTX_ERR_WORKSPACE;

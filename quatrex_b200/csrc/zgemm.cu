@@ -385,6 +385,11 @@ int zgemm(const GemmDesc& d, cudaStream_t s) {
     if (dd.A.null()) dd.A = dd.C.null() ? dd.C3 : dd.C;
     if (dd.B.null()) dd.B = dd.A;
   }
+  if (dd.K > 0 && gemm_slices() > 0 && oz_supported(dd.K, gemm_slices())) {
+    size_t bytes = 0;
+    void* scr = oz_bound(&bytes);
+    if (scr != nullptr) return zgemm_oz(dd, gemm_slices(), scr, bytes, s);
+  }
   const int key = dd.opA * 2 + dd.opB;
   switch (key) {
     case 0: return launch<0, 0>(dd, s);

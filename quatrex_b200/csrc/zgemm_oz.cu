@@ -1,0 +1,737 @@
+// Complex128 GEMM emulated on the int8 tensor cores (tcgen05.mma.kind::i8).
+//
+//   out = alpha op(A) op(B) + sum_t coef_t op_t(D_t)      (the zgemm contract)
+//
+// B200's FP64 tensor rate is a small fraction of its int8 rate, so the FP64
+// products of the RGF and Sancho-Rubio recursions can instead be formed from
+// exact integer products of short slices of the operands (the splitting idea
+// of Ozaki, Ogita, Oishi and Rump, Numer. Algorithms 59 (2012), in its
+// integer-tensor-core form):
+//
+// * Complex -> real. Rows of op(A) interleave (re, im) along k (A', M x 2K);
+//   op(B) is expanded to B'' (2N x 2K) with rows 2j = (re, -im) and
+//   2j+1 = (im, re) per k. The even / odd columns of A' B''^T are Re / Im C.
+// * Split (oz_split_kernel). Every row of A' and every row pair of B'' gets
+//   a power-of-two scale 2^e with all |x| < 2^e; x 2^(L-e), L = 8S - 2, is
+//   rounded to an integer X (|X| <= 2^L) and written as S balanced base-256
+//   digits, X = sum_p D_p 256^(S-1-p), D_p in [-128, 127] (the leading one in
+//   [-65, 65]). Digit p of every element forms int8 plane p (K-major rows,
+//   zero-padded to the tile grid).
+// * Products (oz_gemm_kernel). sum_k X_ik Y_jk = sum_{p,q} 256^(2S-2-p-q)
+//   (D_p E_q^T)_ij. The pairs with p + q = d < S are summed exactly into int32
+//   TMEM accumulator d (|D E| <= 2^14; S * 2K * 2^14 < 2^31 is checked); the
+//   pairs with p + q >= S fall below the rounding of X and are dropped: per
+//   32-byte K step that is S(S+1)/2 MMAs of M=128, N=64, K=32.
+// * Epilogue. T = sum_d acc_d 256^(S-1-d) in FP64, times
+//   2^(e_i + f_j - 2L + 8(S-1)), then zgemm's epilogue (alpha, addends, C,
+//   the conjugate-transposed C2, C3).
+//
+// Error per element: below 2 S K 2^(4-8S) max_k|op(A)_ik| max_k|op(B)_kj|
+// (rounding to L bits plus the dropped pairs); measured relative to
+// (|A||B|)_ij it is ~3e-10 at S = 5, ~1e-12 at S = 6, ~7e-15 at S = 7.
+//
+// CTA tile 128 x 64 real columns (32 complex), 64-byte K stages
+// (SWIZZLE_64B K-major planes of all S slices of A and B), 2-4 stages of
+// cp.async, one thread issues the MMAs and commits each stage to an
+// mbarrier that gates the refill of its buffer. Every mbarrier wait is
+// bounded; on a time-out the CTA records the error, skips its epilogue,
+// frees its TMEM and returns.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace qtx {
+
+namespace {
+
+constexpr int TM = 128;                // UMMA M: rows of op(A) per CTA
+constexpr int TN = 64;                 // UMMA N: real output columns per CTA
+constexpr int TNC = TN / 2;            // complex output columns per CTA
+constexpr int KS = 64;                 // int8 K per pipeline stage (64-byte rows)
+constexpr int THREADS = 256;
+constexpr int PLANE_A = TM * KS;       // 8 KB
+constexpr int PLANE_B = TN * KS;       // 4 KB
+constexpr int TILE_LD = TNC + 1;       // epilogue tile row (complex), padded
+constexpr int SPLIT_ROWS = 32;         // op-rows per split CTA
+constexpr int SPLIT_K = 64;            // complex k per split tile
+constexpr long long kWaitLimit = 1ll << 26;
+
+__device__ int g_oz_error = 0;
+
+template <int S>
+struct Cfg {
+  static constexpr int STAGE = S * (PLANE_A + PLANE_B);
+  static constexpr int NS = (220 * 1024) / STAGE >= 4 ? 4 : (220 * 1024) / STAGE;
+  static constexpr int TMEM_COLS = S * TN <= 256 ? 256 : 512;
+  static constexpr int L = 8 * S - 2;
+  static_assert(S >= 3 && S <= 8, "slice count");
+  static_assert(NS >= 2, "at least two stages");
+  static_assert(TM * TILE_LD * 16 <= NS * STAGE, "epilogue tile must fit the stages");
+};
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// Padded geometry of one call: rows of A', complex columns of op(B), K.
+struct Geom {
+  int Mp, Np, Kc, Kp;
+  size_t item_bytes(int S) const {
+    return sizeof(int) * (size_t)(Mp + Np) + (size_t)S * (size_t)(Mp + 2 * Np) * Kp;
+  }
+};
+Geom geom(int M, int N, int K) {
+  Geom g;
+  g.Mp = round_up(std::max(M, 1), TM);
+  g.Np = round_up(std::max(N, 1), TNC);
+  g.Kc = round_up(std::max(K, 1), KS / 2);
+  g.Kp = 2 * g.Kc;
+  return g;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Byte offset of 16-byte chunk `ch` (0-3) of `row` in a SWIZZLE_64B K-major
+// tile: 8-row groups of 512 B, chunk index XOR ((row / 2) % 4).
+__device__ __forceinline__ uint32_t sw64_offset(int row, int ch) {
+  return (uint32_t)((row >> 3) * 512 + (row & 7) * 64 + ((ch ^ ((row >> 1) & 3)) << 4));
+}
+
+// UMMA shared-memory descriptor, K-major SWIZZLE_64B, 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;           // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;  // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;           // descriptor version (sm_100)
+  d |= (uint64_t)4 << 61;           // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: D s32, A/B s8, K-major both, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+// 2^s as a double for -1022 <= s <= 1023 (exact).
+__device__ __forceinline__ double pow2(int s) { return __longlong_as_double((long long)(s + 1023) << 52); }
+// x 2^s, exactly as scalbn, with one multiply where 2^s and the result are normal.
+__device__ __forceinline__ double ldexp_fast(double x, int s) {
+  return (s >= -1000 && s <= 1000) ? x * pow2(s) : scalbn(x, s);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity));
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+      smem_addr(bar)));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Biased exponent field of |x| (0 for zero and subnormals).
+__device__ __forceinline__ int exp_bits(double x) {
+  return (int)((__double_as_longlong(x) >> 52) & 0x7FF);
+}
+// Scale exponent e with |x| < 2^e for every x of a row whose largest
+// exponent field is eb.
+__device__ __forceinline__ int scale_exp(int eb) { return eb > 0 ? eb - 1022 : -1022; }
+
+// ---------------------------------------------------------------------------
+// Split: one CTA per SPLIT_ROWS op-rows of one batch entry. Sweep 1 finds
+// each row's scale exponent, sweep 2 (whose reads hit L2) writes the digit
+// planes. STRIDED: consecutive op-rows are adjacent in memory (op-row r,
+// index k at X[k ld + r]); otherwise k is contiguous (X[r ld + k]).
+// ---------------------------------------------------------------------------
+struct SplitArgs {
+  MatRef X;
+  int rows, K;  // logical op-rows and depth
+  int conj;
+  int rows_p, Kc, Kp;
+  int64_t b0, bc;
+  int* expo;       // [bc][rows_p] biased exponent fields
+  int8_t* planes;  // [S][bc][prows][Kp], prows = rows_p (A) or 2 rows_p (B)
+  const int* active;
+};
+
+template <int S, bool ISB, bool STRIDED>
+__global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a) {
+  constexpr int L = 8 * S - 2;
+  __shared__ double2 tile[SPLIT_ROWS][SPLIT_K + 1];
+  __shared__ int red[8][SPLIT_ROWS];
+  __shared__ int rexp[SPLIT_ROWS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = blockIdx.x * SPLIT_ROWS;
+  const int bl = blockIdx.y;
+  const int64_t b = a.b0 + bl;
+  if (a.active != nullptr && a.active[b] == 0) return;
+  const double2* X = at<const double2>(a.X, b);
+  const double sgn = a.conj ? -1.0 : 1.0;
+
+  // Sweep 1: the largest exponent field of each op-row.
+  if (STRIDED) {
+    // lanes along rows, warps along k
+    const int r = r0 + lane;
+    int m = 0;
+    if (r < a.rows)
+#pragma unroll 4
+      for (int k = warp; k < a.K; k += 8) {
+        const double2 v = X[(int64_t)k * a.X.ld + r];
+        m = max(m, max(exp_bits(v.x), exp_bits(v.y)));
+      }
+    red[warp][lane] = m;
+    __syncthreads();
+    if (warp == 0) {
+      int mm = red[0][lane];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) mm = max(mm, red[w][lane]);
+      rexp[lane] = mm;
+    }
+  } else {
+    // one warp per row, lanes along k
+    for (int rr = warp; rr < SPLIT_ROWS; rr += 8) {
+      const int r = r0 + rr;
+      int m = 0;
+      if (r < a.rows)
+#pragma unroll 4
+        for (int k = lane; k < a.K; k += 32) {
+          const double2 v = X[(int64_t)r * a.X.ld + k];
+          m = max(m, max(exp_bits(v.x), exp_bits(v.y)));
+        }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) rexp[rr] = m;
+    }
+  }
+  __syncthreads();
+  if (tid < SPLIT_ROWS) a.expo[(int64_t)bl * a.rows_p + r0 + tid] = rexp[tid];
+
+  // Sweep 2: digits, SPLIT_K complex k at a time through shared memory. The
+  // tile stores k at column perm(k) = 8 (k % 8) + k / 8, so the 8 lanes that
+  // read 8 consecutive k each hit distinct banks.
+  const int rr = tid >> 3;       // op-row of this thread
+  const int kc = (tid & 7) * 8;  // first of its 8 k in the tile
+  const int e = scale_exp(rexp[rr]);
+  const int sx = L - e;  // x 2^sx is the integer X before rounding
+  const bool fast = sx >= -1000 && sx <= 1000;
+  const double fx = fast ? pow2(sx) : 0.0;
+  const int prows = ISB ? 2 * a.rows_p : a.rows_p;
+  const size_t plane = (size_t)a.bc * prows * a.Kp;
+  for (int k0 = 0; k0 < a.Kc; k0 += SPLIT_K) {
+    __syncthreads();
+    if (STRIDED) {
+      for (int i = warp; i < SPLIT_K; i += 8) {
+        const int k = k0 + i, r = r0 + lane;
+        double2 v = make_double2(0.0, 0.0);
+        if (k < a.K && r < a.rows) v = X[(int64_t)k * a.X.ld + r];
+        tile[lane][8 * (i & 7) + (i >> 3)] = v;
+      }
+    } else {
+      for (int i = warp; i < SPLIT_ROWS; i += 8) {
+        const int r = r0 + i;
+#pragma unroll
+        for (int j = lane; j < SPLIT_K; j += 32) {
+          const int k = k0 + j;
+          double2 v = make_double2(0.0, 0.0);
+          if (k < a.K && r < a.rows) v = X[(int64_t)r * a.X.ld + k];
+          tile[i][8 * (j & 7) + (j >> 3)] = v;
+        }
+      }
+    }
+    __syncthreads();
+    const int kb = k0 + kc;
+    if (kb >= a.Kc) continue;
+    // xn: -X_im with its own digit chain (balanced digits of -X are not the
+    // negated digits of X where a digit is -128).
+    long long xr[8], xi[8], xn[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double2 v = tile[rr][8 * j + (kc >> 3)];  // k = kc + j
+      xr[j] = __double2ll_rn(fast ? v.x * fx : scalbn(v.x, sx));
+      xi[j] = __double2ll_rn(fast ? sgn * v.y * fx : scalbn(sgn * v.y, sx));
+      xn[j] = -xi[j];
+    }
+    // Digit planes, least significant first; each slice is 16 bytes per row.
+    const int row = r0 + rr;
+#pragma unroll
+    for (int p = S - 1; p >= 0; --p) {
+      uint32_t w0[4], w1[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w0[q] = w1[q] = 0u;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        int dr, di, dn = 0;
+        if (p > 0) {
+          dr = (int)((xr[j] & 0xFF) ^ 0x80) - 0x80;
+          di = (int)((xi[j] & 0xFF) ^ 0x80) - 0x80;
+        } else {
+          dr = (int)xr[j];
+          di = (int)xi[j];
+        }
+        if (ISB) dn = p > 0 ? (int)((xn[j] & 0xFF) ^ 0x80) - 0x80 : (int)xn[j];
+        const int sh = (j & 1) * 16;
+        if (ISB) {
+          w0[j >> 1] |= ((uint32_t)(dr & 0xFF) | ((uint32_t)(dn & 0xFF) << 8)) << sh;
+          w1[j >> 1] |= ((uint32_t)(di & 0xFF) | ((uint32_t)(dr & 0xFF) << 8)) << sh;
+        } else {
+          w0[j >> 1] |= ((uint32_t)(dr & 0xFF) | ((uint32_t)(di & 0xFF) << 8)) << sh;
+        }
+        if (p > 0) {
+          xr[j] = (xr[j] - dr) >> 8;
+          xi[j] = (xi[j] - di) >> 8;
+          if (ISB) xn[j] = (xn[j] - dn) >> 8;
+        }
+      }
+      int8_t* base = a.planes + (size_t)p * plane + (size_t)bl * prows * a.Kp + 2 * (size_t)kb;
+      const uint4 v0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+      if (ISB) {
+        const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+        *reinterpret_cast<uint4*>(base + (size_t)(2 * row) * a.Kp) = v0;
+        *reinterpret_cast<uint4*>(base + (size_t)(2 * row + 1) * a.Kp) = v1;
+      } else {
+        *reinterpret_cast<uint4*>(base + (size_t)row * a.Kp) = v0;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Products and epilogue.
+// ---------------------------------------------------------------------------
+struct GArgs {
+  int M, N, Mp, Np, Kp;
+  int64_t b0, bc;
+  int na, nb;  // plane batch entries of A / B: bc, or 1 for an operand broadcast over the batch
+  const int8_t* pa;  // [S][bc][Mp][Kp]
+  const int8_t* pb;  // [S][bc][2 Np][Kp]
+  const int* ea;     // [bc][Mp]
+  const int* eb;     // [bc][Np]
+  z64 alpha;
+  Addend add[kMaxAddends];
+  int nadd, nadd3;
+  MatRef C, C2, C3;
+  z64 coef2, scale3;
+  const int* active;
+};
+
+__device__ __forceinline__ z64 addend_at(const GArgs& a, int t, int64_t b, int r, int c) {
+  const Addend& ad = a.add[t];
+  const z64* p = at<const z64>(ad.m, b);
+  const z64 x = ad.conj_trans ? zconj(p[(int64_t)c * ad.m.ld + r]) : p[(int64_t)r * ad.m.ld + c];
+  return zmul(ad.coef, x);
+}
+
+// The MMAs of one 64-byte K stage. The S group accumulators lie side by side
+// in TMEM (group d in columns [64 d, 64 d + 64)) and the B slices side by
+// side in shared memory, so A slice p times the stack of B slices
+// 0..S-1-p lands on groups p..S-1 in one instruction of N = 64 (S - p),
+// split at N = 256: each pair (p, q) with p + q < S is formed exactly once.
+template <int S>
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t sb, bool first) {
+#pragma unroll
+  for (int kk = 0; kk < KS / 32; ++kk) {
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
+      const uint64_t da = make_desc(sa + p * PLANE_A + kk * 32);
+#pragma unroll
+      for (int g0 = 0; g0 < S - p; g0 += 4) {
+        constexpr int kMaxGroups = 4;  // N <= 256
+        const int ng = (S - p - g0) < kMaxGroups ? (S - p - g0) : kMaxGroups;
+        const uint64_t db = make_desc(sb + g0 * PLANE_B + kk * 32);
+        mma_i8(tmem + (uint32_t)((p + g0) * TN), da, db, idesc_i8(ng * TN),
+               (first && kk == 0 && p == 0) ? 0u : 1u);
+      }
+    }
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
+  using C = Cfg<S>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::NS * C::STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + C::NS);
+  int* s_ea = reinterpret_cast<int*>(tmem_slot + 4);  // [TM] row scale exponents (biased)
+  int* s_eb = s_ea + TM;                              // [TNC] column scale exponents
+  z64* tile = reinterpret_cast<z64*>(smem);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nr0 = blockIdx.x * TN;  // first B'' row (real output column)
+  const int m0 = blockIdx.y * TM;
+  const int bl = blockIdx.z;
+  const int64_t b = a.b0 + bl;
+  if (a.active != nullptr && a.active[b] == 0) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(C::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < C::NS; ++i) mbar_init(&bar[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  const int ba = a.na > 1 ? bl : 0, bb = a.nb > 1 ? bl : 0;  // plane entries of this batch entry
+  if (tid < TM) s_ea[tid] = a.ea[(int64_t)ba * a.Mp + m0 + tid];
+  else if (tid < TM + TNC) s_eb[tid - TM] = a.eb[(int64_t)bb * a.Np + nr0 / 2 + tid - TM];
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+
+  const size_t sliceA = (size_t)a.na * a.Mp * a.Kp;
+  const size_t sliceB = (size_t)a.nb * 2 * a.Np * a.Kp;
+  const int8_t* ga = a.pa + ((size_t)ba * a.Mp + m0) * a.Kp;
+  const int8_t* gb = a.pb + ((size_t)bb * 2 * a.Np + nr0) * a.Kp;
+  const int nkb = a.Kp / KS;
+
+  auto load_stage = [&](int kb, int buf) {
+    const uint32_t st = smem_addr(smem + buf * C::STAGE);
+#pragma unroll 1
+    for (int t = tid; t < S * (TM + TN) * 4; t += THREADS) {
+      const int ch = t & 3;
+      if (t < S * TM * 4) {
+        const int p = t / (TM * 4), row = (t >> 2) & (TM - 1);
+        cp_async16(st + p * PLANE_A + sw64_offset(row, ch),
+                   ga + p * sliceA + (size_t)row * a.Kp + kb * KS + ch * 16);
+      } else {
+        const int u = t - S * TM * 4;
+        const int p = u / (TN * 4), row = (u >> 2) & (TN - 1);
+        cp_async16(st + S * PLANE_A + p * PLANE_B + sw64_offset(row, ch),
+                   gb + p * sliceB + (size_t)row * a.Kp + kb * KS + ch * 16);
+      }
+    }
+  };
+
+#pragma unroll
+  for (int i = 0; i < C::NS - 1; ++i) {
+    if (i < nkb) load_stage(i, i);
+    cp_async_commit();
+  }
+  bool ok = true;
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int buf = kb % C::NS;
+    cp_async_wait<C::NS - 2>();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t sa = smem_addr(smem + buf * C::STAGE);
+      issue_stage<S>(tmem, sa, sa + S * PLANE_A, kb == 0);
+      mma_commit(&bar[buf]);
+    }
+    const int nk = kb + C::NS - 1;
+    if (nk < nkb) {
+      const int nbuf = nk % C::NS;
+      if (kb >= 1) {
+        // the MMAs of stage kb-1 read buffer nbuf
+        if (tid == 0 && !mbar_wait(&bar[nbuf], (uint32_t)((kb - 1) / C::NS) & 1u)) ok = false;
+        if (!__syncthreads_and(ok)) {
+          ok = false;
+          break;
+        }
+      }
+      load_stage(nk, nbuf);
+    }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  if (ok && nkb > 0) {
+    const int last = nkb - 1;
+    if (tid == 0 && !mbar_wait(&bar[last % C::NS], (uint32_t)(last / C::NS) & 1u)) ok = false;
+  }
+  ok = __syncthreads_and(ok);
+
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    // Phase A: lane = tile row (TMEM lane quarter of warp w is w % 4), warps
+    // 0-3 / 4-7 take real columns 0-31 / 32-63. Digit groups are combined
+    // in FP64, scaled, multiplied by alpha; conjugate-transposed addends.
+    const int wl = warp & 3;
+    const int rl = wl * 32 + lane;
+    const int r = m0 + rl;
+    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+    // row part of the scale: T 2^(e_r + f_c - 2L + 8(S-1))
+    const int er = scale_exp(s_ea[rl]) - 2 * C::L + 8 * (S - 1);
+    int n_ct = 0;
+    for (int t = 0; t < a.nadd; ++t) n_ct += a.add[t].conj_trans;
+#pragma unroll 1
+    for (int c0 = (warp >> 2) * (TN / 2); c0 < (warp >> 2) * (TN / 2) + TN / 2; c0 += 8) {
+      uint32_t v[S][8];
+#pragma unroll
+      for (int d = 0; d < S; ++d)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+            : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
+              "=r"(v[d][6]), "=r"(v[d][7])
+            : "r"(lane_base + (uint32_t)(d * TN + c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+      double T[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        T[j] = (double)(int)v[0][j];
+#pragma unroll
+        for (int d = 1; d < S; ++d) T[j] = fma(T[j], 256.0, (double)(int)v[d][j]);
+      }
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int cl = c0 / 2 + jj;
+        const int c = nr0 / 2 + cl;
+        const int sh = er + scale_exp(s_eb[cl]);
+        z64 z = zmul(a.alpha, make_double2(ldexp_fast(T[2 * jj], sh), ldexp_fast(T[2 * jj + 1], sh)));
+        if (n_ct > 0 && r < a.M && c < a.N)
+          for (int t = 0; t < a.nadd; ++t)
+            if (a.add[t].conj_trans) z = zadd(z, addend_at(a, t, b, r, c));
+        tile[rl * TILE_LD + cl] = z;
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+
+    // Phase B (lane = tile column): the other addends, C3 and C.
+    const int n0 = nr0 / 2;
+#pragma unroll 1
+    for (int e = tid; e < TM * TNC; e += THREADS) {
+      const int rl2 = e / TNC, cl = e % TNC;
+      const int rr = m0 + rl2, c = n0 + cl;
+      if (rr >= a.M || c >= a.N) continue;
+      z64 v = tile[rl2 * TILE_LD + cl];
+      for (int t = 0; t < a.nadd; ++t)
+        if (!a.add[t].conj_trans) v = zadd(v, addend_at(a, t, b, rr, c));
+      if (!a.C3.null()) {
+        z64 v3 = zmul(a.scale3, v);
+        for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) v3 = zadd(v3, addend_at(a, t, b, rr, c));
+        at<z64>(a.C3, b)[(int64_t)rr * a.C3.ld + c] = v3;
+      }
+      if (!a.C.null()) at<z64>(a.C, b)[(int64_t)rr * a.C.ld + c] = v;
+      if (!a.C2.null()) tile[rl2 * TILE_LD + cl] = v;
+    }
+    // Phase C (lane = tile row): the conjugate-transposed store C2.
+    if (!a.C2.null()) {
+      __syncthreads();
+#pragma unroll 1
+      for (int e = tid; e < TM * TNC; e += THREADS) {
+        const int rl2 = e % TM, cl = e / TM;
+        const int rr = m0 + rl2, c = n0 + cl;
+        if (rr >= a.M || c >= a.N) continue;
+        at<z64>(a.C2, b)[(int64_t)c * a.C2.ld + rr] = zmul(a.coef2, zconj(tile[rl2 * TILE_LD + cl]));
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_oz_error, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(C::TMEM_COLS));
+}
+
+// Thread-local GEMM path and bound scratch.
+thread_local int t_slices = 0;
+thread_local void* t_scratch = nullptr;
+thread_local size_t t_scratch_bytes = 0;
+
+template <int S>
+int run_split(const MatRef& X, int rows, int K, int conj, bool isb, bool strided, const Geom& g,
+              int rows_p, int64_t b0, int64_t bc, int* expo, int8_t* planes, const int* active,
+              cudaStream_t s) {
+  SplitArgs a{};
+  a.X = X;
+  a.rows = rows;
+  a.K = K;
+  a.conj = conj;
+  a.rows_p = rows_p;
+  a.Kc = g.Kc;
+  a.Kp = g.Kp;
+  a.b0 = b0;
+  a.bc = bc;
+  a.expo = expo;
+  a.planes = planes;
+  a.active = active;
+  dim3 grid(rows_p / SPLIT_ROWS, (unsigned)bc);
+  if (isb) {
+    if (strided)
+      oz_split_kernel<S, true, true><<<grid, THREADS, 0, s>>>(a);
+    else
+      oz_split_kernel<S, true, false><<<grid, THREADS, 0, s>>>(a);
+  } else {
+    if (strided)
+      oz_split_kernel<S, false, true><<<grid, THREADS, 0, s>>>(a);
+    else
+      oz_split_kernel<S, false, false><<<grid, THREADS, 0, s>>>(a);
+  }
+  QTX_CHECK_LAUNCH();
+  return QTX_OK;
+}
+
+// Digit planes of the batch chunk [b0, b0 + n): [ea][eb] exponents, then the
+// A and B planes. An operand with batch stride 0 (one matrix for every
+// entry, e.g. the coupling blocks) is split once per chunk.
+template <int S>
+int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
+  using C = Cfg<S>;
+  const Geom g = geom(d.M, d.N, d.K);
+  const bool bca = d.A.stride == 0, bcb = d.B.stride == 0;
+  const size_t a_item = sizeof(int) * (size_t)g.Mp + (size_t)S * g.Mp * g.Kp;
+  const size_t b_item = sizeof(int) * (size_t)g.Np + (size_t)S * 2 * g.Np * g.Kp;
+  const size_t fixed = (bca ? a_item : 0) + (bcb ? b_item : 0) + 1024;
+  const size_t per = (bca ? 0 : a_item) + (bcb ? 0 : b_item);
+  int64_t bc = std::min<int64_t>(d.batch, 65535);
+  if (per > 0 && bytes < fixed + per * (size_t)bc) bc = bytes > fixed ? (int64_t)((bytes - fixed) / per) : 0;
+  if (bc <= 0 || bytes < fixed) {
+    set_error("zgemm (int8 emulation): scratch too small for one batch entry");
+    return QTX_ERR_WORKSPACE;
+  }
+  const size_t smem = (size_t)C::NS * C::STAGE + 1024 + 128 + sizeof(int) * (TM + TNC);
+  QTX_CHECK_CUDA(cudaFuncSetAttribute(oz_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int64_t b0 = 0; b0 < d.batch; b0 += bc) {
+    const int64_t n = std::min<int64_t>(bc, d.batch - b0);
+    const int64_t na = bca ? 1 : n, nb = bcb ? 1 : n;
+    char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(scratch) + 255) & ~uintptr_t(255));
+    int* ea = reinterpret_cast<int*>(base);
+    int* eb = ea + (size_t)na * g.Mp;
+    int8_t* pa = reinterpret_cast<int8_t*>(base + ((sizeof(int) * ((size_t)na * g.Mp + (size_t)nb * g.Np) + 255) & ~size_t(255)));
+    int8_t* pb = pa + (size_t)S * na * g.Mp * g.Kp;
+    {
+      ProfScope prof(QTX_KERNEL_SPLIT, 16.0 * ((double)d.M * na + (double)d.N * nb) * d.K, s, 2);
+      QTX_TRY(run_split<S>(d.A, d.M, d.K, d.opA, false, d.opA == 1, g, g.Mp, bca ? 0 : b0, na, ea, pa,
+                           bca ? nullptr : d.active, s));
+      QTX_TRY(run_split<S>(d.B, d.N, d.K, d.opB, true, d.opB == 0, g, g.Np, bcb ? 0 : b0, nb, eb, pb,
+                           bcb ? nullptr : d.active, s));
+    }
+    GArgs a{};
+    a.M = d.M;
+    a.N = d.N;
+    a.Mp = g.Mp;
+    a.Np = g.Np;
+    a.Kp = g.Kp;
+    a.b0 = b0;
+    a.bc = n;
+    a.na = (int)na;
+    a.nb = (int)nb;
+    a.pa = pa;
+    a.pb = pb;
+    a.ea = ea;
+    a.eb = eb;
+    a.alpha = d.alpha;
+    for (int t = 0; t < kMaxAddends; ++t) a.add[t] = d.add[t];
+    a.nadd = d.nadd;
+    a.nadd3 = d.nadd3;
+    a.C = d.C;
+    a.C2 = d.C2;
+    a.C3 = d.C3;
+    a.coef2 = d.coef2;
+    a.scale3 = d.scale3;
+    a.active = d.active;
+    dim3 grid(2 * g.Np / TN, g.Mp / TM, (unsigned)n);
+    ProfScope prof(QTX_KERNEL_ZGEMM_EMU, 8.0 * d.M * d.N * (double)d.K * (double)n, s);
+    oz_gemm_kernel<S><<<grid, THREADS, smem, s>>>(a);
+    QTX_CHECK_LAUNCH();
+  }
+  return QTX_OK;
+}
+
+}  // namespace
+
+size_t oz_scratch_bytes(int M, int N, int K, int64_t batch, int slices) {
+  if (slices <= 0 || batch <= 0) return 0;
+  const Geom g = geom(M, N, K);
+  return g.item_bytes(slices) * (size_t)std::min<int64_t>(batch, 65535) + 1024;
+}
+
+bool oz_supported(int K, int slices) {
+  // S digit pairs of |D E| <= 2^14 summed over 2K must stay inside int32.
+  return slices >= 3 && slices <= 8 && (double)slices * 2.0 * K * 16384.0 < 2147483648.0;
+}
+
+int zgemm_oz(const GemmDesc& d, int slices, void* scratch, size_t bytes, cudaStream_t s) {
+  if (!oz_supported(d.K, slices)) {
+    set_error("zgemm (int8 emulation): slice count outside 3-8 or K too large for int32 sums");
+    return QTX_ERR_ARG;
+  }
+  switch (slices) {
+    case 3: return run<3>(d, scratch, bytes, s);
+    case 4: return run<4>(d, scratch, bytes, s);
+    case 5: return run<5>(d, scratch, bytes, s);
+    case 6: return run<6>(d, scratch, bytes, s);
+    case 7: return run<7>(d, scratch, bytes, s);
+    default: return run<8>(d, scratch, bytes, s);
+  }
+}
+
+void set_gemm_slices(int slices) { t_slices = slices; }
+int gemm_slices() { return t_slices; }
+
+void oz_bind(void* scratch, size_t bytes) {
+  t_scratch = scratch;
+  t_scratch_bytes = bytes;
+}
+void* oz_bound(size_t* bytes) {
+  if (bytes) *bytes = t_scratch_bytes;
+  return t_scratch;
+}
+
+OzScope::OzScope(Workspace& ws, int n, int64_t batch) {
+  prev_p = t_scratch;
+  prev_bytes = t_scratch_bytes;
+  if (t_slices > 0 && n > 0) {
+    const size_t bytes = oz_scratch_bytes(n, n, n, batch, t_slices);
+    void* p = ws.take(bytes);
+    t_scratch = p;
+    t_scratch_bytes = p ? bytes : 0;
+  }
+}
+OzScope::~OzScope() {
+  t_scratch = prev_p;
+  t_scratch_bytes = prev_bytes;
+}
+
+int oz_status_take(int* flag) {
+  int h = 0;
+  QTX_CHECK_CUDA(cudaMemcpyFromSymbol(&h, g_oz_error, sizeof(int)));
+  if (h) {
+    const int zero = 0;
+    QTX_CHECK_CUDA(cudaMemcpyToSymbol(g_oz_error, &zero, sizeof(int)));
+  }
+  *flag = h;
+  return QTX_OK;
+}
+
+}  // namespace qtx

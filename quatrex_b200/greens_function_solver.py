@@ -18,6 +18,7 @@ import torch
 from . import _native
 from ._interop import BTView, default_device, from_device, kind, obc_mats
 from ._native import NULL_MAT, QtxMat
+from .emulation import gemm_path
 from .utils import get_batches, workspace_pool
 
 
@@ -66,20 +67,33 @@ class RGF(GFSolver):
         the reference (default 100).
     device : torch.device, optional
         CUDA device; defaults to the current device.
-    precision : "fp64" (default) or "mixed"
+    precision : "fp64" (default), "mixed" or "emulated"
         "mixed": ``selected_solve`` runs on complex64 copies of the blocks with
         split-TF32 tensor-core products and FP64 inverses of the Schur
         complements (``qtx_selected_solve_mixed``); inputs and outputs keep
         the containers' complex128 type. ``selected_inv`` is always FP64.
+        "emulated": complex128 throughout, every product formed on the int8
+        tensor cores from ``slices`` digit planes per operand (FP64-class
+        accuracy: ~1e-12 relative per product at 6 slices, FP64 level at 7).
+        "fp64" and "mixed" use the FP64 DMMA products whatever GEMM path the
+        calling thread selected with ``emulation.gemm_path``.
+    slices : int
+        Digit planes per operand of the "emulated" precision (3-8).
     """
 
     def __init__(self, max_batch_size: int = 100, device: torch.device | None = None,
-                 precision: str = "fp64") -> None:
-        if precision not in ("fp64", "mixed"):
-            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+                 precision: str = "fp64", slices: int = 6) -> None:
+        if precision not in ("fp64", "mixed", "emulated"):
+            raise ValueError(f"precision must be 'fp64', 'mixed' or 'emulated', got {precision!r}")
+        if precision == "emulated" and not 3 <= int(slices) <= 8:
+            raise ValueError(f"slices must be 3-8, got {slices}")
         self.max_batch_size = max_batch_size
         self.device = device
         self.precision = precision
+        self.slices = int(slices)
+
+    def _path(self):
+        return gemm_path(self.slices if self.precision == "emulated" else 0)
 
     def _dev(self) -> torch.device:
         return self.device if self.device is not None else default_device()
@@ -87,6 +101,10 @@ class RGF(GFSolver):
     # ------------------------------------------------------------------
     def selected_inv(self, a, obc_blocks: OBCBlocks | None = None, out=None):
         """rgf.py:25-113: diagonal and first off-diagonal blocks of A^{-1}."""
+        with self._path():
+            return self._selected_inv(a, obc_blocks, out)
+
+    def _selected_inv(self, a, obc_blocks, out):
         lib = _native.load()
         device = self._dev()
         n = int(a.num_blocks)
@@ -120,6 +138,12 @@ class RGF(GFSolver):
                        return_current: bool = False):
         """rgf.py:115-438: X^R, X^< and X^> on the block-tridiagonal pattern,
         optionally with the Meir-Wingreen layer current."""
+        with self._path():
+            return self._selected_solve(a, sigma_lesser, sigma_greater, obc_blocks, out, return_retarded,
+                                        return_current)
+
+    def _selected_solve(self, a, sigma_lesser, sigma_greater, obc_blocks, out, return_retarded,
+                        return_current):
         lib = _native.load()
         device = self._dev()
         n = int(sigma_lesser.num_blocks)
@@ -288,7 +312,7 @@ def _solve_call(lib, precision, abi, obcs, cur, info, ws_getter, flags, batch, s
     outputs back into the views."""
     n = abi[0].num_blocks
     bs = [int(abi[0].block_sizes[i]) for i in range(n)]
-    if precision == "fp64":
+    if precision in ("fp64", "emulated"):  # the caller's scope selects the GEMM path
         ws = ws_getter(lib.qtx_selected_solve_workspace(n, abi[0].block_sizes, batch, int(cur is not None)))
         _native.check(lib.qtx_selected_solve(
             ctypes.byref(abi[0]), ctypes.byref(abi[1]), ctypes.byref(abi[2]), obcs[0], obcs[1], obcs[2],

@@ -34,6 +34,7 @@ import torch
 from . import _native
 from ._interop import mat
 from ._native import NULL_MAT, QtxBT, QtxMat
+from .emulation import gemm_path
 from .obc import SanchoRubio
 from .utils import WorkspacePool
 
@@ -80,8 +81,14 @@ class EnergyPointSolver:
         Run Sancho-Rubio with device-side convergence (no host
         synchronisation; required for CUDA-graph capture). The host-driven
         loop (default) stops at exactly the reference's iteration.
-    precision : "fp64" or "mixed"
+    precision : "fp64", "mixed" or "emulated"
         "fp64": complex128 throughout (FP64 DMMA products).
+        "emulated": complex128 throughout; the products of the selected
+        solve are formed on the int8 tensor cores from ``slices`` digit
+        planes per operand (``emulation.py``; ~1e-12 relative per product at
+        6 slices, FP64 level at 7). The boundary conditions stay on FP64
+        DMMA products: the Sancho-Rubio doubling recursion amplifies product
+        errors by orders of magnitude.
         "mixed": the boundary conditions (Sancho-Rubio, refinement, contact
         self-energies) stay FP64; the selected solve stores complex64 blocks
         and runs its products on tcgen05 as split-TF32 products with FP32
@@ -104,10 +111,14 @@ class EnergyPointSolver:
                  sr_max_iterations: int = 100, per_energy: bool = True,
                  skip_zero_scattering: bool = False, device: torch.device | None = None,
                  precision: str = "fp64", device_loop: bool = False, store_blocks: bool = True,
-                 potential=None):
-        if precision not in ("fp64", "mixed"):
-            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+                 potential=None, slices: int = 6):
+        if precision not in ("fp64", "mixed", "emulated"):
+            raise ValueError(f"precision must be 'fp64', 'mixed' or 'emulated', got {precision!r}")
+        if precision == "emulated" and not 3 <= int(slices) <= 8:
+            raise ValueError(f"slices must be 3-8, got {slices}")
         self.precision = precision
+        # GEMM path of the library calls: 0 = FP64 DMMA, else int8 emulation
+        self.slices = int(slices) if precision == "emulated" else 0
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         h = torch.as_tensor(np.asarray(h_diag), dtype=_C128) if not isinstance(h_diag, torch.Tensor) else h_diag
         t = torch.as_tensor(np.asarray(coupling), dtype=_C128) if not isinstance(coupling, torch.Tensor) else coupling
@@ -182,7 +193,7 @@ class EnergyPointSolver:
     def resident_bytes(self, B: int) -> int:
         """Device bytes this solver holds for batch size B (buffers and
         workspaces), without allocating anything."""
-        return resident_bytes(self.N, self.b, B, self.precision, self.lib, self.store_blocks)
+        return resident_bytes(self.N, self.b, B, self.precision, self.lib, self.store_blocks, self.slices)
 
     def _buffers(self, B: int) -> dict:
         buf = self._bufs.get(B)
@@ -313,6 +324,10 @@ class EnergyPointSolver:
     def _run(self, B: int, device_loop: bool, warm: bool = False) -> PointResult:
         """The kernel sequence of one batch; no host transfers, and no host
         synchronisation when device_loop is set (graph-capturable)."""
+        with gemm_path(0):  # FP64 DMMA unless a step below selects the emulation
+            return self._enqueue(B, device_loop, warm)
+
+    def _enqueue(self, B: int, device_loop: bool, warm: bool) -> PointResult:
         lib, dev = self.lib, self.device
         N, b = self.N, self.b
         buf = self._bufs[B]
@@ -397,11 +412,12 @@ class EnergyPointSolver:
             obc.append(arr)
         wsq = lib.qtx_selected_solve_mixed_workspace if mixed else lib.qtx_selected_solve_workspace
         solve = lib.qtx_selected_solve_mixed if mixed else lib.qtx_selected_solve
-        ws = self._ws.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
-        _native.check(solve(
-            ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
-            ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
-            buf["density"].data_ptr(), 0, B, buf["info"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
+        with gemm_path(self.slices):
+            ws = self._ws.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
+            _native.check(solve(
+                ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
+                ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
+                buf["density"].data_ptr(), 0, B, buf["info"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
 
         # 4. Transmission (FP64 from the corner block).
         g0n = buf["g0n"]
@@ -437,11 +453,19 @@ class EnergyPointSolver:
         self._host_sr = (it.value, bool(conv.value))
 
 
-def resident_bytes(N: int, b: int, B: int, precision: str = "fp64", lib=None, store_blocks: bool = True) -> int:
+def resident_bytes(N: int, b: int, B: int, precision: str = "fp64", lib=None, store_blocks: bool = True,
+                   slices: int = 6) -> int:
     """Device bytes of an EnergyPointSolver(N blocks of b x b) at batch size
     B: the block stacks of EnergyPointSolver._buffers plus the selected-solve,
     Sancho-Rubio and OBC workspaces (sizes from the library's own queries)."""
     lib = lib or _native.load()
+    if precision == "emulated":
+        bs = (ctypes.c_int32 * N)(*([b] * N))
+        with gemm_path(0):
+            base = resident_bytes(N, b, B, "fp64", lib, store_blocks)
+            plain = int(lib.qtx_selected_solve_workspace(N, bs, B, 1))
+        with gemm_path(slices):
+            return base - plain + int(lib.qtx_selected_solve_workspace(N, bs, B, 1))
     bb = b * b
     n1 = max(N - 1, 1)
     osz = 8 if precision == "mixed" else 16
