@@ -15,8 +15,9 @@
 //   a power-of-two scale 2^e with all |x| < 2^e; x 2^(L-e), L = 8S - 2, is
 //   rounded to an integer X (|X| <= 2^L) and written as S balanced base-256
 //   digits, X = sum_p D_p 256^(S-1-p), D_p in [-128, 127] (the leading one in
-//   [-65, 65]). Digit p of every element forms int8 plane p (K-major rows,
-//   zero-padded to the tile grid).
+//   [-65, 65]). Digit p of every element forms int8 plane p, stored as the
+//   GEMM consumes it: one contiguous, already SWIZZLE_64B-ordered block per
+//   (row tile, 64-byte K block), zero-padded to the tile grid.
 // * Products (oz_gemm_kernel). sum_k X_ik Y_jk = sum_{p,q} 256^(2S-2-p-q)
 //   (D_p E_q^T)_ij. The pairs with p + q = d < S are summed exactly into int32
 //   TMEM accumulator d (|D E| <= 2^14; S * 2K * 2^14 < 2^31 is checked); the
@@ -30,12 +31,13 @@
 // (rounding to L bits plus the dropped pairs); measured relative to
 // (|A||B|)_ij it is ~3e-10 at S = 5, ~1e-12 at S = 6, ~7e-15 at S = 7.
 //
-// CTA tile 128 x 64 real columns (32 complex), 64-byte K stages
-// (SWIZZLE_64B K-major planes of all S slices of A and B), 2-4 stages of
-// cp.async, one thread issues the MMAs and commits each stage to an
-// mbarrier that gates the refill of its buffer. Every mbarrier wait is
-// bounded; on a time-out the CTA records the error, skips its epilogue,
-// frees its TMEM and returns.
+// CTA tile 128 x 64 real columns (32 complex); a 64-byte K stage holds the
+// S A blocks and S B blocks (2S bulk copies, no multicast). One producer
+// thread keeps 2-4 stages in flight on full/empty mbarriers; one thread
+// issues the MMAs and commits each stage back to its empty barrier; all
+// warps run the epilogue once the final commit lands. Every mbarrier wait
+// is bounded; on a time-out the CTA records the error, lets its copies and
+// MMAs in flight finish, skips its epilogue, frees its TMEM and returns.
 #include <algorithm>
 
 #include "common.cuh"
@@ -155,13 +157,14 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
       smem_addr(bar)));
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+// Bulk global -> shared copy completing on an mbarrier (no multicast).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
 
 // Biased exponent field of |x| (0 for zero and subnormals).
@@ -189,10 +192,19 @@ struct SplitArgs {
   const int* active;
 };
 
+__device__ __forceinline__ void cp_async16z(uint32_t dst, const void* src, bool pred) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(pred ? 16 : 0));
+}
+
+constexpr int SPLIT_LD = SPLIT_K + 1;                            // tile row (complex), padded
+constexpr int SPLIT_TILE = SPLIT_ROWS * SPLIT_LD;                // complex elements per tile
+constexpr size_t SPLIT_SMEM = 2 * SPLIT_TILE * sizeof(double2);  // two tiles (double buffer)
+
 template <int S, bool ISB, bool STRIDED>
 __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a) {
   constexpr int L = 8 * S - 2;
-  __shared__ double2 tile[SPLIT_ROWS][SPLIT_K + 1];
+  extern __shared__ __align__(16) uint8_t split_smem[];
+  double2* tiles = reinterpret_cast<double2*>(split_smem);  // [2][SPLIT_ROWS][SPLIT_LD]
   __shared__ int red[8][SPLIT_ROWS];
   __shared__ int rexp[SPLIT_ROWS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -203,17 +215,60 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
   const double2* X = at<const double2>(a.X, b);
   const double sgn = a.conj ? -1.0 : 1.0;
 
+  // K tile t of the strip -> shared buffer `buf` (cp.async, zero-filled
+  // outside the matrix); column perm(k) = 8 (k % 8) + k / 8 within a row.
+  auto load_tile = [&](int t, int buf) {
+    double2* tl = tiles + buf * SPLIT_TILE;
+    const int k0 = t * SPLIT_K;
+    if (STRIDED) {
+#pragma unroll
+      for (int i = warp; i < SPLIT_K; i += 8) {
+        const int k = k0 + i, r = r0 + lane;
+        const bool ok = k < a.K && r < a.rows;
+        cp_async16z(smem_addr(tl + lane * SPLIT_LD + 8 * (i & 7) + (i >> 3)),
+                    ok ? X + (int64_t)k * a.X.ld + r : X, ok);
+      }
+    } else {
+#pragma unroll
+      for (int i = warp; i < SPLIT_ROWS; i += 8) {
+        const int r = r0 + i;
+#pragma unroll
+        for (int j = lane; j < SPLIT_K; j += 32) {
+          const int k = k0 + j;
+          const bool ok = k < a.K && r < a.rows;
+          cp_async16z(smem_addr(tl + i * SPLIT_LD + 8 * (j & 7) + (j >> 3)), ok ? X + (int64_t)r * a.X.ld + k : X,
+                      ok);
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  const int ntiles = (a.Kc + SPLIT_K - 1) / SPLIT_K;
+  load_tile(0, 0);  // in flight during sweep 1
+
   // Sweep 1: the largest exponent field of each op-row.
   if (STRIDED) {
     // lanes along rows, warps along k
     const int r = r0 + lane;
     int m = 0;
-    if (r < a.rows)
-#pragma unroll 4
-      for (int k = warp; k < a.K; k += 8) {
-        const double2 v = X[(int64_t)k * a.X.ld + r];
-        m = max(m, max(exp_bits(v.x), exp_bits(v.y)));
+    if (r < a.rows) {
+      // 8 independent loads in flight per lane
+      int mm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      int k = warp;
+      for (; k + 56 < a.K; k += 64) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const double2 v = X[(int64_t)(k + 8 * u) * a.X.ld + r];
+          mm[u] = max(mm[u], max(exp_bits(v.x), exp_bits(v.y)));
+        }
       }
+      for (; k < a.K; k += 8) {
+        const double2 v = X[(int64_t)k * a.X.ld + r];
+        mm[0] = max(mm[0], max(exp_bits(v.x), exp_bits(v.y)));
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) m = max(m, mm[u]);
+    }
     red[warp][lane] = m;
     __syncthreads();
     if (warp == 0) {
@@ -223,19 +278,28 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
       rexp[lane] = mm;
     }
   } else {
-    // one warp per row, lanes along k
-    for (int rr = warp; rr < SPLIT_ROWS; rr += 8) {
-      const int r = r0 + rr;
-      int m = 0;
-      if (r < a.rows)
-#pragma unroll 4
-        for (int k = lane; k < a.K; k += 32) {
-          const double2 v = X[(int64_t)r * a.X.ld + k];
-          m = max(m, max(exp_bits(v.x), exp_bits(v.y)));
+    // one warp per row, lanes along k; the warp's 4 rows interleaved so that
+    // 4 x 4 independent loads are in flight per lane
+    int m4[4] = {0, 0, 0, 0};
+    for (int k = lane; k < a.K; k += 128) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = r0 + warp + 8 * q, kk = k + 32 * u;
+          if (r < a.rows && kk < a.K) {
+            const double2 v = X[(int64_t)r * a.X.ld + kk];
+            m4[q] = max(m4[q], max(exp_bits(v.x), exp_bits(v.y)));
+          }
         }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int m = m4[q];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if (lane == 0) rexp[rr] = m;
+      if (lane == 0) rexp[warp + 8 * q] = m;
     }
   }
   __syncthreads();
@@ -252,81 +316,83 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
   const double fx = fast ? pow2(sx) : 0.0;
   const int prows = ISB ? 2 * a.rows_p : a.rows_p;
   const size_t plane = (size_t)a.bc * prows * a.Kp;
-  for (int k0 = 0; k0 < a.Kc; k0 += SPLIT_K) {
-    __syncthreads();
-    if (STRIDED) {
-      for (int i = warp; i < SPLIT_K; i += 8) {
-        const int k = k0 + i, r = r0 + lane;
-        double2 v = make_double2(0.0, 0.0);
-        if (k < a.K && r < a.rows) v = X[(int64_t)k * a.X.ld + r];
-        tile[lane][8 * (i & 7) + (i >> 3)] = v;
-      }
+  const int nkb = a.Kp / KS;
+  for (int t = 0; t < ntiles; ++t) {
+    const int k0 = t * SPLIT_K;
+    if (t + 1 < ntiles) {
+      load_tile(t + 1, (t + 1) & 1);  // its buffer was last read before the barrier ending t - 1
+      asm volatile("cp.async.wait_group 1;\n" ::);
     } else {
-      for (int i = warp; i < SPLIT_ROWS; i += 8) {
-        const int r = r0 + i;
-#pragma unroll
-        for (int j = lane; j < SPLIT_K; j += 32) {
-          const int k = k0 + j;
-          double2 v = make_double2(0.0, 0.0);
-          if (k < a.K && r < a.rows) v = X[(int64_t)r * a.X.ld + k];
-          tile[i][8 * (j & 7) + (j >> 3)] = v;
-        }
-      }
+      asm volatile("cp.async.wait_group 0;\n" ::);
     }
     __syncthreads();
+    const double2* tl = tiles + (t & 1) * SPLIT_TILE;
     const int kb = k0 + kc;
-    if (kb >= a.Kc) continue;
-    // xn: -X_im with its own digit chain (balanced digits of -X are not the
-    // negated digits of X where a digit is -128).
-    long long xr[8], xi[8], xn[8];
+    if (kb >= a.Kc) {
+      __syncthreads();
+      continue;
+    }
+    // Balanced base-256 digits (each in [-128, 127]) of X are the bytes of
+    // Z = (X + C) xor C, C = 0x80 in each of the S low bytes: adding C makes
+    // every byte non-negative and xor 0x80 re-centres it. Digit p (most
+    // significant first) is byte S-1-p. -X_im gets its own Z (its digits are
+    // not the negated digits of X_im where one is -128).
+    constexpr unsigned long long kC = 0x8080808080808080ull >> (8 * (8 - S));
+    uint32_t zr[8][2], zi[8][2], zn[8][2];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const double2 v = tile[rr][8 * j + (kc >> 3)];  // k = kc + j
-      xr[j] = __double2ll_rn(fast ? v.x * fx : scalbn(v.x, sx));
-      xi[j] = __double2ll_rn(fast ? sgn * v.y * fx : scalbn(sgn * v.y, sx));
-      xn[j] = -xi[j];
+      const double2 v = tl[rr * SPLIT_LD + 8 * j + (kc >> 3)];  // k = kc + j
+      const long long xr = __double2ll_rn(fast ? v.x * fx : scalbn(v.x, sx));
+      const long long xi = __double2ll_rn(fast ? sgn * v.y * fx : scalbn(sgn * v.y, sx));
+      const unsigned long long ur = ((unsigned long long)xr + kC) ^ kC;
+      const unsigned long long ui = ((unsigned long long)xi + kC) ^ kC;
+      zr[j][0] = (uint32_t)ur, zr[j][1] = (uint32_t)(ur >> 32);
+      zi[j][0] = (uint32_t)ui, zi[j][1] = (uint32_t)(ui >> 32);
+      if (ISB) {
+        const unsigned long long un = ((unsigned long long)(-xi) + kC) ^ kC;
+        zn[j][0] = (uint32_t)un, zn[j][1] = (uint32_t)(un >> 32);
+      }
     }
-    // Digit planes, least significant first; each slice is 16 bytes per row.
     const int row = r0 + rr;
 #pragma unroll
-    for (int p = S - 1; p >= 0; --p) {
+    for (int p = 0; p < S; ++p) {
+      const int bi = S - 1 - p;          // byte of Z holding digit p
+      const int hw = bi >> 2;            // its 32-bit half
+      const uint32_t sel = (uint32_t)(bi & 3);
+      const uint32_t pair = sel | ((4u + sel) << 4);  // byte sel of x, byte sel of y
       uint32_t w0[4], w1[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) w0[q] = w1[q] = 0u;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        int dr, di, dn = 0;
-        if (p > 0) {
-          dr = (int)((xr[j] & 0xFF) ^ 0x80) - 0x80;
-          di = (int)((xi[j] & 0xFF) ^ 0x80) - 0x80;
-        } else {
-          dr = (int)xr[j];
-          di = (int)xi[j];
-        }
-        if (ISB) dn = p > 0 ? (int)((xn[j] & 0xFF) ^ 0x80) - 0x80 : (int)xn[j];
-        const int sh = (j & 1) * 16;
+      for (int q = 0; q < 4; ++q) {
+        const int j0 = 2 * q, j1 = 2 * q + 1;
         if (ISB) {
-          w0[j >> 1] |= ((uint32_t)(dr & 0xFF) | ((uint32_t)(dn & 0xFF) << 8)) << sh;
-          w1[j >> 1] |= ((uint32_t)(di & 0xFF) | ((uint32_t)(dr & 0xFF) << 8)) << sh;
+          // row 2j: (re, -im); row 2j+1: (im, re)
+          w0[q] = __byte_perm(__byte_perm(zr[j0][hw], zn[j0][hw], pair), __byte_perm(zr[j1][hw], zn[j1][hw], pair),
+                              0x5410);
+          w1[q] = __byte_perm(__byte_perm(zi[j0][hw], zr[j0][hw], pair), __byte_perm(zi[j1][hw], zr[j1][hw], pair),
+                              0x5410);
         } else {
-          w0[j >> 1] |= ((uint32_t)(dr & 0xFF) | ((uint32_t)(di & 0xFF) << 8)) << sh;
-        }
-        if (p > 0) {
-          xr[j] = (xr[j] - dr) >> 8;
-          xi[j] = (xi[j] - di) >> 8;
-          if (ISB) xn[j] = (xn[j] - dn) >> 8;
+          w0[q] = __byte_perm(__byte_perm(zr[j0][hw], zi[j0][hw], pair), __byte_perm(zr[j1][hw], zi[j1][hw], pair),
+                              0x5410);
+          w1[q] = 0u;
         }
       }
-      int8_t* base = a.planes + (size_t)p * plane + (size_t)bl * prows * a.Kp + 2 * (size_t)kb;
+      // plane block (p, entry, row tile, K block) as the GEMM stages load it
+      const int col = 2 * kb;  // byte column: one 16-byte swizzle chunk
+      const size_t kblk = (size_t)(col / KS), ch = (size_t)((col % KS) / 16);
+      int8_t* ptile = a.planes + (size_t)p * plane + (size_t)bl * prows * a.Kp;
       const uint4 v0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
       if (ISB) {
         const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
-        *reinterpret_cast<uint4*>(base + (size_t)(2 * row) * a.Kp) = v0;
-        *reinterpret_cast<uint4*>(base + (size_t)(2 * row + 1) * a.Kp) = v1;
+        const int r2 = 2 * row;
+        int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN, (int)ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN + 1, (int)ch)) = v1;
       } else {
-        *reinterpret_cast<uint4*>(base + (size_t)row * a.Kp) = v0;
+        int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(row % TM, (int)ch)) = v0;
       }
     }
+    __syncthreads();  // buffer t & 1 is refilled at iteration t + 1
   }
 }
 
@@ -385,8 +451,10 @@ __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
   using C = Cfg<S>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::NS * C::STAGE);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + C::NS);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NS * C::STAGE);  // stage loaded
+  uint64_t* empty = full + C::NS;                                             // stage consumed by the MMAs
+  uint64_t* done = empty + C::NS;                                             // all MMAs complete
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   int* s_ea = reinterpret_cast<int*>(tmem_slot + 4);  // [TM] row scale exponents (biased)
   int* s_eb = s_ea + TM;                              // [TNC] column scale exponents
   z64* tile = reinterpret_cast<z64*>(smem);
@@ -404,8 +472,12 @@ __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
                  "r"(C::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
-  if (tid == 0) {
-    for (int i = 0; i < C::NS; ++i) mbar_init(&bar[i], 1);
+  if (tid == 32) {
+    for (int i = 0; i < C::NS; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
   const int ba = a.na > 1 ? bl : 0, bb = a.nb > 1 ? bl : 0;  // plane entries of this batch entry
@@ -416,66 +488,54 @@ __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
 
-  const size_t sliceA = (size_t)a.na * a.Mp * a.Kp;
-  const size_t sliceB = (size_t)a.nb * 2 * a.Np * a.Kp;
-  const int8_t* ga = a.pa + ((size_t)ba * a.Mp + m0) * a.Kp;
-  const int8_t* gb = a.pb + ((size_t)bb * 2 * a.Np + nr0) * a.Kp;
+  // Plane block (p, entry, tile, K block) is contiguous and pre-swizzled.
   const int nkb = a.Kp / KS;
+  const int MT = a.Mp / TM, NT = 2 * a.Np / TN;
+  const int8_t* ga = a.pa + ((size_t)ba * MT + blockIdx.y) * nkb * PLANE_A;
+  const int8_t* gb = a.pb + ((size_t)bb * NT + blockIdx.x) * nkb * PLANE_B;
+  const size_t sliceA = (size_t)a.na * MT * nkb * PLANE_A;
+  const size_t sliceB = (size_t)a.nb * NT * nkb * PLANE_B;
 
-  auto load_stage = [&](int kb, int buf) {
-    const uint32_t st = smem_addr(smem + buf * C::STAGE);
-#pragma unroll 1
-    for (int t = tid; t < S * (TM + TN) * 4; t += THREADS) {
-      const int ch = t & 3;
-      if (t < S * TM * 4) {
-        const int p = t / (TM * 4), row = (t >> 2) & (TM - 1);
-        cp_async16(st + p * PLANE_A + sw64_offset(row, ch),
-                   ga + p * sliceA + (size_t)row * a.Kp + kb * KS + ch * 16);
-      } else {
-        const int u = t - S * TM * 4;
-        const int p = u / (TN * 4), row = (u >> 2) & (TN - 1);
-        cp_async16(st + S * PLANE_A + p * PLANE_B + sw64_offset(row, ch),
-                   gb + p * sliceB + (size_t)row * a.Kp + kb * KS + ch * 16);
-      }
-    }
-  };
-
-#pragma unroll
-  for (int i = 0; i < C::NS - 1; ++i) {
-    if (i < nkb) load_stage(i, i);
-    cp_async_commit();
-  }
   bool ok = true;
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int buf = kb % C::NS;
-    cp_async_wait<C::NS - 2>();
-    asm volatile("fence.proxy.async.shared::cta;\n" ::);
-    __syncthreads();
-    if (tid == 0) {
+  if (warp == 1 && lane == 0) {
+    // Producer: 2S bulk copies per stage onto full[buf], once the MMAs of the
+    // stage that used the buffer before have released it (empty[buf]).
+    int issued = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int buf = kb % C::NS;
+      const uint32_t u = (uint32_t)(kb / C::NS);
+      if (kb >= C::NS && !mbar_wait(&empty[buf], (u - 1u) & 1u)) {
+        ok = false;
+        break;
+      }
+      const uint32_t st = smem_addr(smem + buf * C::STAGE);
+      expect_tx(&full[buf], (uint32_t)C::STAGE);
+#pragma unroll
+      for (int p = 0; p < S; ++p)
+        bulk_g2s(st + p * PLANE_A, ga + p * sliceA + (size_t)kb * PLANE_A, PLANE_A, &full[buf]);
+#pragma unroll
+      for (int q = 0; q < S; ++q)
+        bulk_g2s(st + S * PLANE_A + q * PLANE_B, gb + q * sliceB + (size_t)kb * PLANE_B, PLANE_B, &full[buf]);
+      issued = kb + 1;
+    }
+    if (!ok)  // let the copies in flight land before the CTA exits
+      for (int kb = issued > C::NS ? issued - C::NS : 0; kb < issued; ++kb)
+        mbar_wait(&full[kb % C::NS], (uint32_t)(kb / C::NS) & 1u);
+  } else if (warp == 0 && lane == 0) {
+    // MMA issuer: consumes the stages in order; tcgen05.commit releases each.
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int buf = kb % C::NS;
+      if (!mbar_wait(&full[buf], (uint32_t)(kb / C::NS) & 1u)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       const uint32_t sa = smem_addr(smem + buf * C::STAGE);
       issue_stage<S>(tmem, sa, sa + S * PLANE_A, kb == 0);
-      mma_commit(&bar[buf]);
+      mma_commit(&empty[buf]);
     }
-    const int nk = kb + C::NS - 1;
-    if (nk < nkb) {
-      const int nbuf = nk % C::NS;
-      if (kb >= 1) {
-        // the MMAs of stage kb-1 read buffer nbuf
-        if (tid == 0 && !mbar_wait(&bar[nbuf], (uint32_t)((kb - 1) / C::NS) & 1u)) ok = false;
-        if (!__syncthreads_and(ok)) {
-          ok = false;
-          break;
-        }
-      }
-      load_stage(nk, nbuf);
-    }
-    cp_async_commit();
-  }
-  cp_async_wait<0>();
-  if (ok && nkb > 0) {
-    const int last = nkb - 1;
-    if (tid == 0 && !mbar_wait(&bar[last % C::NS], (uint32_t)(last / C::NS) & 1u)) ok = false;
+    mma_commit(done);  // tracks every MMA issued above, on either path
+    if (!mbar_wait(done, 0)) ok = false;
   }
   ok = __syncthreads_and(ok);
 
@@ -586,16 +646,15 @@ int run_split(const MatRef& X, int rows, int K, int conj, bool isb, bool strided
   a.planes = planes;
   a.active = active;
   dim3 grid(rows_p / SPLIT_ROWS, (unsigned)bc);
+  auto launch = [&](auto kern) -> int {
+    QTX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SPLIT_SMEM));
+    kern<<<grid, THREADS, SPLIT_SMEM, s>>>(a);
+    return QTX_OK;
+  };
   if (isb) {
-    if (strided)
-      oz_split_kernel<S, true, true><<<grid, THREADS, 0, s>>>(a);
-    else
-      oz_split_kernel<S, true, false><<<grid, THREADS, 0, s>>>(a);
+    QTX_TRY(strided ? launch(oz_split_kernel<S, true, true>) : launch(oz_split_kernel<S, true, false>));
   } else {
-    if (strided)
-      oz_split_kernel<S, false, true><<<grid, THREADS, 0, s>>>(a);
-    else
-      oz_split_kernel<S, false, false><<<grid, THREADS, 0, s>>>(a);
+    QTX_TRY(strided ? launch(oz_split_kernel<S, false, true>) : launch(oz_split_kernel<S, false, false>));
   }
   QTX_CHECK_LAUNCH();
   return QTX_OK;
@@ -619,7 +678,7 @@ int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
     set_error("zgemm (int8 emulation): scratch too small for one batch entry");
     return QTX_ERR_WORKSPACE;
   }
-  const size_t smem = (size_t)C::NS * C::STAGE + 1024 + 128 + sizeof(int) * (TM + TNC);
+  const size_t smem = (size_t)C::NS * C::STAGE + 1024 + 256 + sizeof(int) * (TM + TNC);
   QTX_CHECK_CUDA(cudaFuncSetAttribute(oz_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int64_t b0 = 0; b0 < d.batch; b0 += bc) {
     const int64_t n = std::min<int64_t>(bc, d.batch - b0);
