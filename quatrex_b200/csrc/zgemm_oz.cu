@@ -396,6 +396,138 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Split, strip form: one CTA per STRIP_ROWS op-rows of one batch entry with
+// the whole K strip staged in shared memory by one wave of cp.async, so the
+// operand is read from HBM once; exponents and digits come from the copy.
+// Within a row, complex k sits at strip_pos(k): 256-element segments with
+// k % 8 major, so the 32 lanes that each take 8 consecutive k read distinct
+// banks. Used for padded K from 512 up to STRIP_MAX_KC.
+// ---------------------------------------------------------------------------
+constexpr int STRIP_ROWS = 8;
+constexpr int STRIP_MAX_KC = 1792;  // 8 rows x 1792 x 16 B = 224 KB
+
+__device__ __forceinline__ int strip_pos(int k) { return (k & ~255) | ((k & 7) << 5) | ((k >> 3) & 31); }
+
+__host__ __device__ inline int strip_len(int Kc) { return (Kc + 255) / 256 * 256; }
+
+template <int S, bool ISB, bool STRIDED>
+__global__ void __launch_bounds__(THREADS, 2) oz_split_strip_kernel(const SplitArgs a) {
+  constexpr int L = 8 * S - 2;
+  extern __shared__ __align__(16) uint8_t split_smem[];
+  double2* strip = reinterpret_cast<double2*>(split_smem);  // [STRIP_ROWS][KL]
+  __shared__ int rexp[STRIP_ROWS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = blockIdx.x * STRIP_ROWS;
+  const int bl = blockIdx.y;
+  const int64_t b = a.b0 + bl;
+  if (a.active != nullptr && a.active[b] == 0) return;
+  const double2* X = at<const double2>(a.X, b);
+  const double sgn = a.conj ? -1.0 : 1.0;
+  const int KL = strip_len(a.Kc);  // padded row length (zero-filled past K)
+
+  if (STRIDED) {
+    // the 8 op-rows of one k are adjacent: 8 lanes per k, 32 k per pass
+    const int i = tid & 7, r = r0 + i;
+    for (int k = tid >> 3; k < KL; k += THREADS / 8) {
+      const bool ok = k < a.K && r < a.rows;
+      cp_async16z(smem_addr(strip + i * KL + strip_pos(k)), ok ? X + (int64_t)k * a.X.ld + r : X, ok);
+    }
+  } else {
+    const int r = r0 + warp;  // warp w loads row w
+    for (int k = lane; k < KL; k += 32) {
+      const bool ok = k < a.K && r < a.rows;
+      cp_async16z(smem_addr(strip + warp * KL + strip_pos(k)), ok ? X + (int64_t)r * a.X.ld + k : X, ok);
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+
+  // Row scale exponent: warp w reduces row w.
+  const double2* row_s = strip + warp * KL;
+  {
+    int m = 0;
+    for (int q = lane; q < KL; q += 32) {
+      const double2 v = row_s[q];
+      m = max(m, max(exp_bits(v.x), exp_bits(v.y)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) {
+      rexp[warp] = m;
+      a.expo[(int64_t)bl * a.rows_p + r0 + warp] = m;
+    }
+  }
+  __syncwarp();
+  const int e = scale_exp(rexp[warp]);
+  const int sx = L - e;
+  const bool fast = sx >= -1000 && sx <= 1000;
+  const double fx = fast ? pow2(sx) : 0.0;
+  const int prows = ISB ? 2 * a.rows_p : a.rows_p;
+  const size_t plane = (size_t)a.bc * prows * a.Kp;
+  const int nkb = a.Kp / KS;
+  const int row = r0 + warp;
+  constexpr unsigned long long kC = 0x8080808080808080ull >> (8 * (8 - S));
+
+  // Digits: lane l takes chunks c = l, l + 32, ... of 8 consecutive k.
+  for (int c = lane; c < a.Kc / 8; c += 32) {
+    uint32_t zr[8][2], zi[8][2], zn[8][2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double2 v = row_s[(c >> 5) * 256 + 32 * j + (c & 31)];  // k = 8c + j
+      const long long xr = __double2ll_rn(fast ? v.x * fx : scalbn(v.x, sx));
+      const long long xi = __double2ll_rn(fast ? sgn * v.y * fx : scalbn(sgn * v.y, sx));
+      const unsigned long long ur = ((unsigned long long)xr + kC) ^ kC;
+      const unsigned long long ui = ((unsigned long long)xi + kC) ^ kC;
+      zr[j][0] = (uint32_t)ur, zr[j][1] = (uint32_t)(ur >> 32);
+      zi[j][0] = (uint32_t)ui, zi[j][1] = (uint32_t)(ui >> 32);
+      if (ISB) {
+        const unsigned long long un = ((unsigned long long)(-xi) + kC) ^ kC;
+        zn[j][0] = (uint32_t)un, zn[j][1] = (uint32_t)(un >> 32);
+      }
+    }
+    const int col = 16 * c;  // byte column of the chunk: one 16-byte swizzle chunk
+    const size_t kblk = (size_t)(col / KS);
+    const int ch = (col % KS) / 16;
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
+      const int bi = S - 1 - p;
+      const int hw = bi >> 2;
+      const uint32_t sel = (uint32_t)(bi & 3);
+      const uint32_t pair = sel | ((4u + sel) << 4);
+      uint32_t w0[4], w1[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j0 = 2 * q, j1 = 2 * q + 1;
+        if (ISB) {
+          w0[q] = __byte_perm(__byte_perm(zr[j0][hw], zn[j0][hw], pair), __byte_perm(zr[j1][hw], zn[j1][hw], pair),
+                              0x5410);
+          w1[q] = __byte_perm(__byte_perm(zi[j0][hw], zr[j0][hw], pair), __byte_perm(zi[j1][hw], zr[j1][hw], pair),
+                              0x5410);
+        } else {
+          w0[q] = __byte_perm(__byte_perm(zr[j0][hw], zi[j0][hw], pair), __byte_perm(zr[j1][hw], zi[j1][hw], pair),
+                              0x5410);
+          w1[q] = 0u;
+        }
+      }
+      int8_t* ptile = a.planes + (size_t)p * plane + (size_t)bl * prows * a.Kp;
+      const uint4 v0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+      if (ISB) {
+        const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+        const int r2 = 2 * row;
+        int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN, ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN + 1, ch)) = v1;
+      } else {
+        int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
+        *reinterpret_cast<uint4*>(blk + sw64_offset(row % TM, ch)) = v0;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Products and epilogue.
 // ---------------------------------------------------------------------------
@@ -645,6 +777,25 @@ int run_split(const MatRef& X, int rows, int K, int conj, bool isb, bool strided
   a.expo = expo;
   a.planes = planes;
   a.active = active;
+  if (strip_len(g.Kc) >= 512 && strip_len(g.Kc) <= STRIP_MAX_KC) {
+    // whole K strips in shared memory: one HBM read of the operand (measured
+    // faster than the two-sweep form from K = 512 on, slower below)
+    const size_t smem = (size_t)STRIP_ROWS * strip_len(g.Kc) * sizeof(double2);
+    dim3 grid(rows_p / STRIP_ROWS, (unsigned)bc);
+    auto launch = [&](auto kern) -> int {
+      QTX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<grid, THREADS, smem, s>>>(a);
+      return QTX_OK;
+    };
+    if (isb) {
+      QTX_TRY(strided ? launch(oz_split_strip_kernel<S, true, true>) : launch(oz_split_strip_kernel<S, true, false>));
+    } else {
+      QTX_TRY(strided ? launch(oz_split_strip_kernel<S, false, true>)
+                      : launch(oz_split_strip_kernel<S, false, false>));
+    }
+    QTX_CHECK_LAUNCH();
+    return QTX_OK;
+  }
   dim3 grid(rows_p / SPLIT_ROWS, (unsigned)bc);
   auto launch = [&](auto kern) -> int {
     QTX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SPLIT_SMEM));
