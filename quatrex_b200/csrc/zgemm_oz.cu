@@ -578,6 +578,88 @@ __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t
   }
 }
 
+// Epilogue, part 1 (lane = tile row rl = 32 wl + lane; TMEM lane quarter
+// wl): real columns [c_lo, c_hi) of the S digit-group accumulators are
+// combined in FP64, scaled by 2^(e_r + f_c - 2L + 8(S-1)), multiplied by
+// alpha, the conjugate-transposed addends added, and the complex results
+// written to the shared tile.
+template <int S>
+__device__ __forceinline__ void epilogue_tmem(const GArgs& a, uint32_t tmem, z64* tile, const int* s_ea,
+                                              const int* s_eb, int64_t b, int m0, int nr0, int wl, int lane,
+                                              int c_lo, int c_hi) {
+  constexpr int L = 8 * S - 2;
+  const int rl = wl * 32 + lane;
+  const int r = m0 + rl;
+  const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+  const int er = scale_exp(s_ea[rl]) - 2 * L + 8 * (S - 1);
+  int n_ct = 0;
+  for (int t = 0; t < a.nadd; ++t) n_ct += a.add[t].conj_trans;
+#pragma unroll 1
+  for (int c0 = c_lo; c0 < c_hi; c0 += 8) {
+    uint32_t v[S][8];
+#pragma unroll
+    for (int d = 0; d < S; ++d)
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+          : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
+            "=r"(v[d][6]), "=r"(v[d][7])
+          : "r"(lane_base + (uint32_t)(d * TN + c0)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+    double T[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      T[j] = (double)(int)v[0][j];
+#pragma unroll
+      for (int d = 1; d < S; ++d) T[j] = fma(T[j], 256.0, (double)(int)v[d][j]);
+    }
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int cl = c0 / 2 + jj;
+      const int c = nr0 / 2 + cl;
+      const int sh = er + scale_exp(s_eb[cl]);
+      z64 z = zmul(a.alpha, make_double2(ldexp_fast(T[2 * jj], sh), ldexp_fast(T[2 * jj + 1], sh)));
+      if (n_ct > 0 && r < a.M && c < a.N)
+        for (int t = 0; t < a.nadd; ++t)
+          if (a.add[t].conj_trans) z = zadd(z, addend_at(a, t, b, r, c));
+      tile[rl * TILE_LD + cl] = z;
+    }
+  }
+}
+
+// Epilogue, part 2 (lane = tile column, threads t0.. of nt): the other
+// addends, C3 and C; the tile keeps the primary result for C2.
+__device__ __forceinline__ void epilogue_rows(const GArgs& a, z64* tile, int64_t b, int m0, int n0, int t0,
+                                              int nt) {
+#pragma unroll 1
+  for (int e = t0; e < TM * TNC; e += nt) {
+    const int rl = e / TNC, cl = e % TNC;
+    const int rr = m0 + rl, c = n0 + cl;
+    if (rr >= a.M || c >= a.N) continue;
+    z64 v = tile[rl * TILE_LD + cl];
+    for (int t = 0; t < a.nadd; ++t)
+      if (!a.add[t].conj_trans) v = zadd(v, addend_at(a, t, b, rr, c));
+    if (!a.C3.null()) {
+      z64 v3 = zmul(a.scale3, v);
+      for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) v3 = zadd(v3, addend_at(a, t, b, rr, c));
+      at<z64>(a.C3, b)[(int64_t)rr * a.C3.ld + c] = v3;
+    }
+    if (!a.C.null()) at<z64>(a.C, b)[(int64_t)rr * a.C.ld + c] = v;
+    if (!a.C2.null()) tile[rl * TILE_LD + cl] = v;
+  }
+}
+
+// Epilogue, part 3 (lane = tile row): the conjugate-transposed store C2.
+__device__ __forceinline__ void epilogue_c2(const GArgs& a, const z64* tile, int64_t b, int m0, int n0, int t0,
+                                            int nt) {
+#pragma unroll 1
+  for (int e = t0; e < TM * TNC; e += nt) {
+    const int rl = e % TM, cl = e / TM;
+    const int rr = m0 + rl, c = n0 + cl;
+    if (rr >= a.M || c >= a.N) continue;
+    at<z64>(a.C2, b)[(int64_t)c * a.C2.ld + rr] = zmul(a.coef2, zconj(tile[rl * TILE_LD + cl]));
+  }
+}
+
 template <int S>
 __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
   using C = Cfg<S>;
@@ -674,77 +756,15 @@ __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     // Phase A: lane = tile row (TMEM lane quarter of warp w is w % 4), warps
-    // 0-3 / 4-7 take real columns 0-31 / 32-63. Digit groups are combined
-    // in FP64, scaled, multiplied by alpha; conjugate-transposed addends.
-    const int wl = warp & 3;
-    const int rl = wl * 32 + lane;
-    const int r = m0 + rl;
-    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
-    // row part of the scale: T 2^(e_r + f_c - 2L + 8(S-1))
-    const int er = scale_exp(s_ea[rl]) - 2 * C::L + 8 * (S - 1);
-    int n_ct = 0;
-    for (int t = 0; t < a.nadd; ++t) n_ct += a.add[t].conj_trans;
-#pragma unroll 1
-    for (int c0 = (warp >> 2) * (TN / 2); c0 < (warp >> 2) * (TN / 2) + TN / 2; c0 += 8) {
-      uint32_t v[S][8];
-#pragma unroll
-      for (int d = 0; d < S; ++d)
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-            : "=r"(v[d][0]), "=r"(v[d][1]), "=r"(v[d][2]), "=r"(v[d][3]), "=r"(v[d][4]), "=r"(v[d][5]),
-              "=r"(v[d][6]), "=r"(v[d][7])
-            : "r"(lane_base + (uint32_t)(d * TN + c0)));
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-      double T[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        T[j] = (double)(int)v[0][j];
-#pragma unroll
-        for (int d = 1; d < S; ++d) T[j] = fma(T[j], 256.0, (double)(int)v[d][j]);
-      }
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int cl = c0 / 2 + jj;
-        const int c = nr0 / 2 + cl;
-        const int sh = er + scale_exp(s_eb[cl]);
-        z64 z = zmul(a.alpha, make_double2(ldexp_fast(T[2 * jj], sh), ldexp_fast(T[2 * jj + 1], sh)));
-        if (n_ct > 0 && r < a.M && c < a.N)
-          for (int t = 0; t < a.nadd; ++t)
-            if (a.add[t].conj_trans) z = zadd(z, addend_at(a, t, b, r, c));
-        tile[rl * TILE_LD + cl] = z;
-      }
-    }
+    // 0-3 / 4-7 take real columns 0-31 / 32-63.
+    epilogue_tmem<S>(a, tmem, tile, s_ea, s_eb, b, m0, nr0, warp & 3, lane, (warp >> 2) * (TN / 2),
+                     (warp >> 2) * (TN / 2) + TN / 2);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
-
-    // Phase B (lane = tile column): the other addends, C3 and C.
-    const int n0 = nr0 / 2;
-#pragma unroll 1
-    for (int e = tid; e < TM * TNC; e += THREADS) {
-      const int rl2 = e / TNC, cl = e % TNC;
-      const int rr = m0 + rl2, c = n0 + cl;
-      if (rr >= a.M || c >= a.N) continue;
-      z64 v = tile[rl2 * TILE_LD + cl];
-      for (int t = 0; t < a.nadd; ++t)
-        if (!a.add[t].conj_trans) v = zadd(v, addend_at(a, t, b, rr, c));
-      if (!a.C3.null()) {
-        z64 v3 = zmul(a.scale3, v);
-        for (int t = a.nadd; t < a.nadd + a.nadd3; ++t) v3 = zadd(v3, addend_at(a, t, b, rr, c));
-        at<z64>(a.C3, b)[(int64_t)rr * a.C3.ld + c] = v3;
-      }
-      if (!a.C.null()) at<z64>(a.C, b)[(int64_t)rr * a.C.ld + c] = v;
-      if (!a.C2.null()) tile[rl2 * TILE_LD + cl] = v;
-    }
-    // Phase C (lane = tile row): the conjugate-transposed store C2.
+    epilogue_rows(a, tile, b, m0, nr0 / 2, tid, THREADS);
     if (!a.C2.null()) {
       __syncthreads();
-#pragma unroll 1
-      for (int e = tid; e < TM * TNC; e += THREADS) {
-        const int rl2 = e % TM, cl = e / TM;
-        const int rr = m0 + rl2, c = n0 + cl;
-        if (rr >= a.M || c >= a.N) continue;
-        at<z64>(a.C2, b)[(int64_t)c * a.C2.ld + rr] = zmul(a.coef2, zconj(tile[rl2 * TILE_LD + cl]));
-      }
+      epilogue_c2(a, tile, b, m0, nr0 / 2, tid, THREADS);
     }
   } else if (tid == 0) {
     atomicExch(&g_oz_error, 1);
@@ -870,8 +890,8 @@ int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
     a.coef2 = d.coef2;
     a.scale3 = d.scale3;
     a.active = d.active;
-    dim3 grid(2 * g.Np / TN, g.Mp / TM, (unsigned)n);
     ProfScope prof(QTX_KERNEL_ZGEMM_EMU, 8.0 * d.M * d.N * (double)d.K * (double)n, s);
+    dim3 grid(2 * g.Np / TN, g.Mp / TM, (unsigned)n);
     oz_gemm_kernel<S><<<grid, THREADS, smem, s>>>(a);
     QTX_CHECK_LAUNCH();
   }
