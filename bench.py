@@ -54,8 +54,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS peak measurements")
-    p.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
-                   help="fp64 is the headline value; mixed is reported beside it")
+    p.add_argument("--precision", choices=["fp64", "mixed", "emulated", "both"], default="both",
+                   help="fp64 is the headline value; mixed (and emulated) are reported beside it. cfg1 also "
+                        "accepts 'emulated' alone (FP64 with int8-emulated products as the main line)")
     p.add_argument("--emulated-slices", type=int, default=6,
                    help="cfg1 with --precision both: also time the FP64 path with its complex128 products "
                         "emulated on the int8 tensor cores from this many digit planes (0: skip)")
@@ -370,8 +371,10 @@ def run_ours(args, world, rank, local):
     fl_all, fr_all = dev.fermi_left(), dev.fermi_right()
     lib = _native.load()
     peak = {"peak": None} if args.no_peak else measured_fp64_peak(torch, device)
-    tf32_peak = None if (args.no_peak or args.precision == "fp64") else measured_tf32_peak(torch, device)
-    emulate = args.precision == "both" and args.emulated_slices > 0
+    tf32_peak = None if (args.no_peak or args.precision in ("fp64", "emulated")) else measured_tf32_peak(torch, device)
+    emulate = args.precision == "emulated" or (args.precision == "both" and args.emulated_slices > 0)
+    if emulate and not 3 <= args.emulated_slices <= 8:
+        raise SystemExit("--emulated-slices must be 3-8 for the emulated leg")
     int8_peak = measured_int8_peak(torch, device) if (emulate and not args.no_peak) else None
     props = torch.cuda.get_device_properties(device)
     gpu_id = str(getattr(props, "uuid", local))
@@ -447,12 +450,13 @@ def run_ours(args, world, rank, local):
         return ms, prof, clk, sr_iters, probe_out, per_step, prof_ref_ms
 
     res = {}
-    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]) + (["emulated"] if emulate
-                                                                                         else []):
+    precs = ((["fp64", "mixed"] + (["emulated"] if emulate else [])) if args.precision == "both"
+             else [args.precision])
+    for prec in precs:
         res[prec] = timed(prec)
-    main_prec = "fp64" if "fp64" in res else "mixed"
+    main_prec = precs[0]
     ms, prof, clk, sr_iters, _, per_step, pms = res[main_prec]
-    gemm_ms, gemm_flops, gemm_n = prof["zgemm"] if main_prec == "fp64" else prof["cgemm"]
+    gemm_ms, gemm_flops, gemm_n = prof[{"fp64": "zgemm", "mixed": "cgemm", "emulated": "zgemm_emu"}[main_prec]]
     inv_ms, inv_flops, inv_n = prof["zinv"]
     all_ms, _, all_n = prof["all"]
 
@@ -572,6 +576,14 @@ def run_ours(args, world, rank, local):
                     "peak_source": "measured cuBLAS FP64 (max of DGEMM 8192^3, ZGEMM 4096^3) on this GPU; "
                                    "no FP64 entry in MEASURED_PEAKS.json",
                     "peak_detail": peak, "traffic": _ncu_traffic(), "launches": gemm_n}
+    elif main_prec == "emulated":
+        S = args.emulated_slices
+        tops = achieved * (S * (S + 1) // 2) if achieved else None  # int8 ops = 8mnk x digit pairs
+        roofline = {"bound": "tensor", "kernel": "oz_gemm_kernel (tcgen05 kind::i8, M=128, N<=256)",
+                    "achieved": tops, "peak": int8_peak, "unit": "int8 TOPS (2 x int8 MACs)",
+                    "frac": (tops / int8_peak) if tops and int8_peak else None,
+                    "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
+                    "fp64_equivalent_tflops": achieved, "traffic": None, "launches": gemm_n}
     else:
         roofline = {"bound": "tensor", "kernel": "cgemm_tc (tcgen05 kind::tf32, 12 MMAs per complex K step)",
                     "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s (complex as-written 8mnk)",
@@ -589,11 +601,13 @@ def run_ours(args, world, rank, local):
     its = np.mean(np.array(sr_iters), axis=0) if sr_iters else (0, 0)
     fl = flops_per_energy(32, 256, tuple(float(x) for x in its))
     line = {
-        "metric": METRIC if main_prec == "fp64" else METRIC.replace("(FP64)", "(mixed)"),
+        "metric": {"fp64": METRIC, "mixed": METRIC.replace("(FP64)", "(mixed)"),
+                   "emulated": METRIC.replace("(FP64)", "(FP64, int8-emulated products)")}[main_prec],
         "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 (complex128)" if main_prec == "fp64" else "c64 storage, split-TF32 products",
+        "dtype": {"fp64": "f64 (complex128)", "mixed": "c64 storage, split-TF32 products",
+                  "emulated": f"f64 (complex128); products from {args.emulated_slices} int8 digit planes"}[main_prec],
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "batch": B, "energies": args.energies,
                    "parallelism": f"energy sharding x{world}", "inverse_path": args.inverse_path,
@@ -962,6 +976,30 @@ def run_kernels(args, local):
     out["cgemm_cublas_bmm_tf32_allowed"] = flops / timeit(lambda: torch.bmm(a32, b32, out=c32)) / 1e12
     torch.backends.cuda.matmul.allow_tf32 = old
     del a32, b32, c32
+    # Complex128 products emulated on the int8 tensor cores (digit planes).
+    from quatrex_b200.emulation import workspace_bytes, zgemm_emulated
+
+    _native.check(lib.qtx_zgemm_batched(n, n, n, B, 1.0, 0.0, mat(a), 0, mat(b), 0, 0.0, 0.0, z, 0, mat(c),
+                                        stream()))
+    ref = c.clone()
+    emu = {}
+    for S in (5, 6, 7):
+        wsS = torch.empty(workspace_bytes(n, n, n, B, S), dtype=torch.uint8, device=device)
+        t = timeit(lambda: zgemm_emulated(a, b, slices=S, out=c, workspace=wsS))
+        lib.qtx_profile_reset()
+        lib.qtx_profile_enable(1)
+        zgemm_emulated(a, b, slices=S, out=c, workspace=wsS)
+        torch.cuda.synchronize()
+        gm, sp = _native.profile_read(6), _native.profile_read(7)
+        lib.qtx_profile_enable(0)
+        emu[f"slices_{S}"] = {
+            "fp64_equivalent_tflops": flops / t / 1e12, "speedup_vs_zgemm_ours": (flops / t / 1e12) / out["zgemm_ours"],
+            "gemm_ms": gm[0], "split_ms": sp[0],
+            "gemm_int8_tops": gm[1] * (S * (S + 1) // 2) / (gm[0] * 1e-3) / 1e12 if gm[0] else None,
+            "rel_err_vs_dmma": float(torch.linalg.norm(c - ref) / torch.linalg.norm(ref))}
+        del wsS
+    out["zgemm_emulated_int8"] = emu
+    del ref
     eye = torch.eye(n, dtype=torch.complex128, device=device)
     w = (a + n * eye).contiguous()  # well conditioned
     info = torch.zeros(B, dtype=torch.int32, device=device)
