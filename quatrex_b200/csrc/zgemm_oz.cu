@@ -49,7 +49,8 @@ namespace {
 constexpr int TM = 128;                // UMMA M: rows of op(A) per CTA
 constexpr int TN = 64;                 // UMMA N: real output columns per CTA
 constexpr int TNC = TN / 2;            // complex output columns per CTA
-constexpr int KS = 64;                 // int8 K per pipeline stage (64-byte rows)
+constexpr int KS = 64;                 // int8 K per pipeline stage (64-byte rows, two MMA K steps;
+                                       // 32-byte stages measured slower)
 constexpr int THREADS = 256;
 constexpr int PLANE_A = TM * KS;       // 8 KB
 constexpr int PLANE_B = TN * KS;       // 4 KB
@@ -93,20 +94,25 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Byte offset of 16-byte chunk `ch` (0-3) of `row` in a SWIZZLE_64B K-major
-// tile: 8-row groups of 512 B, chunk index XOR ((row / 2) % 4).
-__device__ __forceinline__ uint32_t sw64_offset(int row, int ch) {
-  return (uint32_t)((row >> 3) * 512 + (row & 7) * 64 + ((ch ^ ((row >> 1) & 3)) << 4));
+// Byte offset of 16-byte chunk `ch` of `row` in a K-major tile of KS-byte
+// rows, swizzled as the UMMA descriptor below declares: 8-row groups of
+// 8 KS bytes; the chunk index XOR row bits above the 128-byte line
+// (SWIZZLE_32B: chunk ^ (row / 4) % 2; SWIZZLE_64B: chunk ^ (row / 2) % 4).
+__device__ __forceinline__ uint32_t swz_offset(int row, int ch) {
+  const int x = KS == 64 ? ((row >> 1) & 3) : ((row >> 2) & 1);
+  return (uint32_t)((row >> 3) * (8 * KS) + (row & 7) * KS + ((ch ^ x) << 4));
 }
 
-// UMMA shared-memory descriptor, K-major SWIZZLE_64B, 8-row groups 512 B apart.
+// UMMA shared-memory descriptor, K-major, SWIZZLE_32B (KS = 32) or
+// SWIZZLE_64B (KS = 64), 8-row groups 8 KS bytes apart.
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+  static_assert(KS == 32 || KS == 64, "stage rows of 32 or 64 bytes");
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-  d |= (uint64_t)1 << 16;           // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;  // stride byte offset: next 8-row group
-  d |= (uint64_t)1 << 46;           // descriptor version (sm_100)
-  d |= (uint64_t)4 << 61;           // SWIZZLE_64B
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((8 * KS) >> 4) << 32;     // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;                   // descriptor version (sm_100)
+  d |= (uint64_t)(KS == 64 ? 4 : 6) << 61;  // SWIZZLE_64B / SWIZZLE_32B
   return d;
 }
 
@@ -385,11 +391,11 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
         const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
         const int r2 = 2 * row;
         int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN, (int)ch)) = v0;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN + 1, (int)ch)) = v1;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN, (int)ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN + 1, (int)ch)) = v1;
       } else {
         int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(row % TM, (int)ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(row % TM, (int)ch)) = v0;
       }
     }
     __syncthreads();  // buffer t & 1 is refilled at iteration t + 1
@@ -518,11 +524,11 @@ __global__ void __launch_bounds__(THREADS, 2) oz_split_strip_kernel(const SplitA
         const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
         const int r2 = 2 * row;
         int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN, ch)) = v0;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(r2 % TN + 1, ch)) = v1;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN, ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN + 1, ch)) = v1;
       } else {
         int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
-        *reinterpret_cast<uint4*>(blk + sw64_offset(row % TM, ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(row % TM, ch)) = v0;
       }
     }
   }
