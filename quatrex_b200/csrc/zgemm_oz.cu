@@ -11,18 +11,21 @@
 // * Complex -> real. Rows of op(A) interleave (re, im) along k (A', M x 2K);
 //   op(B) is expanded to B'' (2N x 2K) with rows 2j = (re, -im) and
 //   2j+1 = (im, re) per k. The even / odd columns of A' B''^T are Re / Im C.
-// * Split (oz_split_kernel). Every row of A' and every row pair of B'' gets
-//   a power-of-two scale 2^e with all |x| < 2^e; x 2^(L-e), L = 8S - 2, is
-//   rounded to an integer X (|X| <= 2^L) and written as S balanced base-256
-//   digits, X = sum_p D_p 256^(S-1-p), D_p in [-128, 127] (the leading one in
-//   [-65, 65]). Digit p of every element forms int8 plane p, stored as the
-//   GEMM consumes it: one contiguous, already SWIZZLE_64B-ordered block per
+// * Split (oz_split_kernel, oz_split_strip_kernel). Every row of A' and every
+//   row pair of B'' gets a power-of-two scale 2^e with all |x| < 2^e;
+//   x 2^(L-e), L = 8S - 2, is rounded to an integer X (|X| <= 2^L) and written
+//   as S balanced base-256 digits, X = sum_p D_p 256^(S-1-p), D_p in
+//   [-128, 127] (the leading one in [-65, 65]): the bytes of
+//   (X + 0x80..80) xor 0x80..80. Digit p of every element forms int8 plane p,
+//   stored as the GEMM consumes it: one contiguous, already swizzled block per
 //   (row tile, 64-byte K block), zero-padded to the tile grid.
 // * Products (oz_gemm_kernel). sum_k X_ik Y_jk = sum_{p,q} 256^(2S-2-p-q)
 //   (D_p E_q^T)_ij. The pairs with p + q = d < S are summed exactly into int32
 //   TMEM accumulator d (|D E| <= 2^14; S * 2K * 2^14 < 2^31 is checked); the
-//   pairs with p + q >= S fall below the rounding of X and are dropped: per
-//   32-byte K step that is S(S+1)/2 MMAs of M=128, N=64, K=32.
+//   pairs with p + q >= S fall below the rounding of X and are dropped. With
+//   the accumulators side by side in TMEM, A plane p times the stacked B
+//   planes 0..S-1-p is one MMA of M=128, N = 64 (S-p) (split at N = 256)
+//   per 32-byte K step.
 // * Epilogue. T = sum_d acc_d 256^(S-1-d) in FP64, times
 //   2^(e_i + f_j - 2L + 8(S-1)), then zgemm's epilogue (alpha, addends, C,
 //   the conjugate-transposed C2, C3).
