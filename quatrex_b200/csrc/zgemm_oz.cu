@@ -33,6 +33,8 @@
 // Error per element: below 2 S K 2^(4-8S) max_k|op(A)_ik| max_k|op(B)_kj|
 // (rounding to L bits plus the dropped pairs); measured relative to
 // (|A||B|)_ij it is ~3e-10 at S = 5, ~1e-12 at S = 6, ~7e-15 at S = 7.
+// An element whose row of op(A) or column of op(B) holds an Inf or NaN is
+// NaN (the digits of a non-finite value do not exist).
 //
 // CTA tile 128 x 64 real columns (32 complex); a 64-byte K stage holds the
 // S A blocks and S B blocks (2S bulk copies, no multicast). One producer
@@ -627,6 +629,8 @@ __device__ __forceinline__ void epilogue_tmem(const GArgs& a, uint32_t tmem, z64
       const int c = nr0 / 2 + cl;
       const int sh = er + scale_exp(s_eb[cl]);
       z64 z = zmul(a.alpha, make_double2(ldexp_fast(T[2 * jj], sh), ldexp_fast(T[2 * jj + 1], sh)));
+      if (s_ea[rl] == 0x7FF || s_eb[cl] == 0x7FF)  // Inf or NaN in the row / column: no digits
+        z = make_double2(__longlong_as_double(0x7FF8000000000000ll), __longlong_as_double(0x7FF8000000000000ll));
       if (n_ct > 0 && r < a.M && c < a.N)
         for (int t = 0; t < a.nadd; ++t)
           if (a.add[t].conj_trans) z = zadd(z, addend_at(a, t, b, r, c));

@@ -176,3 +176,25 @@ def test_emulated_broadcast_operands(cuda_device):
     C = zgemm_emulated(torch.from_numpy(a1.conj().swapaxes(-1, -2).copy()).to(cuda_device).expand(B, k, m), tb,
                        op_a=1, slices=7)
     _check(C.cpu().numpy(), np.broadcast_to(a1, a.shape), b, 0, 0, 7)
+
+
+def test_emulated_non_finite_inputs_give_nan(cuda_device):
+    """A row of op(A) or a column of op(B) holding Inf / NaN makes its output
+    row / column NaN; everything else is unaffected."""
+    rng = np.random.default_rng(9)
+    a, b = _rand(rng, 2, 40, 50), _rand(rng, 2, 50, 60)
+    a[0, 3, 7] = np.inf
+    b[1, 11, 5] = complex(0.0, np.nan)
+    C = zgemm_emulated(torch.from_numpy(a).to(cuda_device), torch.from_numpy(b).to(cuda_device), slices=6)
+    got = C.cpu().numpy()
+    bad = np.zeros(got.shape, dtype=bool)
+    bad[0, 3, :] = True
+    bad[1, :, 5] = True
+    assert np.all(np.isnan(got[bad]))
+    assert np.all(np.isfinite(got[~bad]))
+    ok_a, ok_b = a.copy(), b.copy()
+    ok_a[0, 3, 7] = 0.0
+    ok_b[1, 11, 5] = 0.0
+    ref = ok_a @ ok_b
+    scale = np.abs(ok_a) @ np.abs(ok_b)
+    assert np.max(np.abs(got - ref)[~bad] / scale[~bad]) < REL[6]
