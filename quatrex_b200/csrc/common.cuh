@@ -119,7 +119,6 @@ int zgemm_oz(const GemmDesc& d, int slices, void* scratch, size_t bytes, cudaStr
 // that many slices (used where a driver bound scratch for it).
 void set_gemm_slices(int slices);
 int gemm_slices();
-void oz_bind(void* scratch, size_t bytes);
 void* oz_bound(size_t* bytes);
 // Reads and clears the device flag of timed-out waits in the emulated GEMM.
 int oz_status_take(int* flag);

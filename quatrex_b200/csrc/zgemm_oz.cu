@@ -942,10 +942,6 @@ int zgemm_oz(const GemmDesc& d, int slices, void* scratch, size_t bytes, cudaStr
 void set_gemm_slices(int slices) { t_slices = slices; }
 int gemm_slices() { return t_slices; }
 
-void oz_bind(void* scratch, size_t bytes) {
-  t_scratch = scratch;
-  t_scratch_bytes = bytes;
-}
 void* oz_bound(size_t* bytes) {
   if (bytes) *bytes = t_scratch_bytes;
   return t_scratch;

@@ -198,3 +198,25 @@ def test_emulated_non_finite_inputs_give_nan(cuda_device):
     ref = ok_a @ ok_b
     scale = np.abs(ok_a) @ np.abs(ok_b)
     assert np.max(np.abs(got - ref)[~bad] / scale[~bad]) < REL[6]
+
+
+def test_sancho_rubio_and_contact_on_emulated_path(cuda_device):
+    """The boundary-condition drivers bind the plane scratch from their own
+    workspace under gemm_path(); at 7 planes they agree with FP64 DMMA."""
+    from quatrex_b200 import SanchoRubio, contact_self_energy, synthetic
+
+    dev = synthetic.make_device(num_blocks=4, block_size=64, energies=np.linspace(-1.0, 1.0, 5), seed=2)
+    d, u, l = dev.system_blocks()
+    a_ii, a_ij, a_ji = (torch.from_numpy(np.ascontiguousarray(x)).to(cuda_device) for x in (d[0], u[0], l[0]))
+    f = torch.from_numpy(dev.fermi_left()).to(cuda_device)
+    sr = SanchoRubio(convergence_tol=1e-12, per_energy=True)
+    g64 = sr(a_ii, a_ij, a_ji, "left")
+    s64 = contact_self_energy(a_ij, a_ji, g64, f)
+    with gemm_path(7):
+        g7 = sr(a_ii, a_ij, a_ji, "left")
+        s7 = contact_self_energy(a_ij, a_ji, g7, f)
+    assert status() == 0
+    rel = float(torch.linalg.norm(g7 - g64) / torch.linalg.norm(g64))
+    assert rel < 1e-8, rel
+    for x7, x64 in zip(s7, s64):
+        assert float(torch.linalg.norm(x7 - x64) / torch.linalg.norm(x64)) < 1e-8
