@@ -52,30 +52,42 @@ namespace qtx {
 namespace {
 
 constexpr int TM = 128;                // UMMA M: rows of op(A) per CTA
-constexpr int TN = 64;                 // UMMA N: real output columns per CTA
-constexpr int TNC = TN / 2;            // complex output columns per CTA
 constexpr int KS = 64;                 // int8 K per pipeline stage (64-byte rows, two MMA K steps;
                                        // 32-byte stages measured slower)
 constexpr int THREADS = 256;
 constexpr int PLANE_A = TM * KS;       // 8 KB
-constexpr int PLANE_B = TN * KS;       // 4 KB
-constexpr int TILE_LD = TNC + 1;       // epilogue tile row (complex), padded
 constexpr int SPLIT_ROWS = 32;         // op-rows per split CTA
 constexpr int SPLIT_K = 64;            // complex k per split tile
 constexpr long long kWaitLimit = 1ll << 26;
 
 __device__ int g_oz_error = 0;
 
+// Per plane count S: the CTA's real output columns TN (UMMA N of one digit
+// group), CTAs per SM and the stage ring. The S int32 accumulator groups take
+// S x TN TMEM columns; at most 256 lets two CTAs share an SM, so that one's
+// loads, barrier round trips and epilogue overlap the other's MMAs (S <= 4 at
+// TN = 64, S = 5 at TN = 48); S >= 6 keeps one CTA per SM with 64 columns.
 template <int S>
 struct Cfg {
+  static constexpr int TN = S == 5 ? 48 : 64;
+  static constexpr int TNC = TN / 2;         // complex output columns per CTA
+  static constexpr int TILE_LD = TNC + 1;    // epilogue tile row (complex), padded
+  static constexpr int PLANE_B = TN * KS;    // one B plane block
+  static constexpr int CPS = S * TN <= 256 ? 2 : 1;
   static constexpr int STAGE = S * (PLANE_A + PLANE_B);
-  static constexpr int NS = (220 * 1024) / STAGE >= 4 ? 4 : (220 * 1024) / STAGE;
+  static constexpr int BUDGET = CPS == 2 ? 110 * 1024 : 220 * 1024;
+  static constexpr int NS = BUDGET / STAGE >= 4 ? 4 : BUDGET / STAGE;
   static constexpr int TMEM_COLS = S * TN <= 256 ? 256 : 512;
   static constexpr int L = 8 * S - 2;
+  static constexpr int GROUPS_PER_MMA = 256 / TN;  // UMMA N <= 256
   static_assert(S >= 3 && S <= 8, "slice count");
   static_assert(NS >= 2, "at least two stages");
   static_assert(TM * TILE_LD * 16 <= NS * STAGE, "epilogue tile must fit the stages");
+  static_assert(TN % 16 == 0 && TN % 8 == 0, "UMMA N granularity");
 };
+
+// Complex output columns per CTA for S planes (the padding unit of op(B)).
+constexpr int tnc_for(int slices) { return slices == 5 ? 24 : 32; }
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -86,10 +98,10 @@ struct Geom {
     return sizeof(int) * (size_t)(Mp + Np) + (size_t)S * (size_t)(Mp + 2 * Np) * Kp;
   }
 };
-Geom geom(int M, int N, int K) {
+Geom geom(int M, int N, int K, int tnc) {
   Geom g;
   g.Mp = round_up(std::max(M, 1), TM);
-  g.Np = round_up(std::max(N, 1), TNC);
+  g.Np = round_up(std::max(N, 1), tnc);
   g.Kc = round_up(std::max(K, 1), KS / 2);
   g.Kp = 2 * g.Kc;
   return g;
@@ -314,7 +326,9 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
     }
   }
   __syncthreads();
-  if (tid < SPLIT_ROWS) a.expo[(int64_t)bl * a.rows_p + r0 + tid] = rexp[tid];
+  // the last CTA may reach past the padded row count (a multiple of the
+  // GEMM's tile, not of SPLIT_ROWS): those rows are neither stored nor read
+  if (tid < SPLIT_ROWS && r0 + tid < a.rows_p) a.expo[(int64_t)bl * a.rows_p + r0 + tid] = rexp[tid];
 
   // Sweep 2: digits, SPLIT_K complex k at a time through shared memory. The
   // tile stores k at column perm(k) = 8 (k % 8) + k / 8, so the 8 lanes that
@@ -339,7 +353,7 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
     __syncthreads();
     const double2* tl = tiles + (t & 1) * SPLIT_TILE;
     const int kb = k0 + kc;
-    if (kb >= a.Kc) {
+    if (kb >= a.Kc || r0 + rr >= a.rows_p) {
       __syncthreads();
       continue;
     }
@@ -395,9 +409,10 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
       if (ISB) {
         const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
         const int r2 = 2 * row;
-        int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN, (int)ch)) = v0;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN + 1, (int)ch)) = v1;
+        constexpr int TNB = Cfg<S>::TN;
+        int8_t* blk = ptile + ((size_t)(r2 / TNB) * nkb + kblk) * Cfg<S>::PLANE_B;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB, (int)ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB + 1, (int)ch)) = v1;
       } else {
         int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
         *reinterpret_cast<uint4*>(blk + swz_offset(row % TM, (int)ch)) = v0;
@@ -528,9 +543,10 @@ __global__ void __launch_bounds__(THREADS, 2) oz_split_strip_kernel(const SplitA
       if (ISB) {
         const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
         const int r2 = 2 * row;
-        int8_t* blk = ptile + ((size_t)(r2 / TN) * nkb + kblk) * PLANE_B;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN, ch)) = v0;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TN + 1, ch)) = v1;
+        constexpr int TNB = Cfg<S>::TN;
+        int8_t* blk = ptile + ((size_t)(r2 / TNB) * nkb + kblk) * Cfg<S>::PLANE_B;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB, ch)) = v0;
+        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB + 1, ch)) = v1;
       } else {
         int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
         *reinterpret_cast<uint4*>(blk + swz_offset(row % TM, ch)) = v0;
@@ -572,17 +588,17 @@ __device__ __forceinline__ z64 addend_at(const GArgs& a, int t, int64_t b, int r
 // split at N = 256: each pair (p, q) with p + q < S is formed exactly once.
 template <int S>
 __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t sb, bool first) {
+  using C = Cfg<S>;
 #pragma unroll
   for (int kk = 0; kk < KS / 32; ++kk) {
 #pragma unroll
     for (int p = 0; p < S; ++p) {
       const uint64_t da = make_desc(sa + p * PLANE_A + kk * 32);
 #pragma unroll
-      for (int g0 = 0; g0 < S - p; g0 += 4) {
-        constexpr int kMaxGroups = 4;  // N <= 256
-        const int ng = (S - p - g0) < kMaxGroups ? (S - p - g0) : kMaxGroups;
-        const uint64_t db = make_desc(sb + g0 * PLANE_B + kk * 32);
-        mma_i8(tmem + (uint32_t)((p + g0) * TN), da, db, idesc_i8(ng * TN),
+      for (int g0 = 0; g0 < S - p; g0 += C::GROUPS_PER_MMA) {
+        const int ng = (S - p - g0) < C::GROUPS_PER_MMA ? (S - p - g0) : C::GROUPS_PER_MMA;
+        const uint64_t db = make_desc(sb + g0 * C::PLANE_B + kk * 32);
+        mma_i8(tmem + (uint32_t)((p + g0) * C::TN), da, db, idesc_i8(ng * C::TN),
                (first && kk == 0 && p == 0) ? 0u : 1u);
       }
     }
@@ -599,6 +615,7 @@ __device__ __forceinline__ void epilogue_tmem(const GArgs& a, uint32_t tmem, z64
                                               const int* s_eb, int64_t b, int m0, int nr0, int wl, int lane,
                                               int c_lo, int c_hi) {
   constexpr int L = 8 * S - 2;
+  constexpr int TN = Cfg<S>::TN, TILE_LD = Cfg<S>::TILE_LD;
   const int rl = wl * 32 + lane;
   const int r = m0 + rl;
   const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
@@ -641,8 +658,10 @@ __device__ __forceinline__ void epilogue_tmem(const GArgs& a, uint32_t tmem, z64
 
 // Epilogue, part 2 (lane = tile column, threads t0.. of nt): the other
 // addends, C3 and C; the tile keeps the primary result for C2.
+template <int S>
 __device__ __forceinline__ void epilogue_rows(const GArgs& a, z64* tile, int64_t b, int m0, int n0, int t0,
                                               int nt) {
+  constexpr int TNC = Cfg<S>::TNC, TILE_LD = Cfg<S>::TILE_LD;
 #pragma unroll 1
   for (int e = t0; e < TM * TNC; e += nt) {
     const int rl = e / TNC, cl = e % TNC;
@@ -662,8 +681,10 @@ __device__ __forceinline__ void epilogue_rows(const GArgs& a, z64* tile, int64_t
 }
 
 // Epilogue, part 3 (lane = tile row): the conjugate-transposed store C2.
+template <int S>
 __device__ __forceinline__ void epilogue_c2(const GArgs& a, const z64* tile, int64_t b, int m0, int n0, int t0,
                                             int nt) {
+  constexpr int TNC = Cfg<S>::TNC, TILE_LD = Cfg<S>::TILE_LD;
 #pragma unroll 1
   for (int e = t0; e < TM * TNC; e += nt) {
     const int rl = e % TM, cl = e / TM;
@@ -674,8 +695,9 @@ __device__ __forceinline__ void epilogue_c2(const GArgs& a, const z64* tile, int
 }
 
 template <int S>
-__global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
+__global__ void __launch_bounds__(THREADS, Cfg<S>::CPS) oz_gemm_kernel(const GArgs a) {
   using C = Cfg<S>;
+  constexpr int TN = C::TN, TNC = C::TNC, PLANE_B = C::PLANE_B;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::NS * C::STAGE);  // stage loaded
@@ -774,10 +796,10 @@ __global__ void __launch_bounds__(THREADS, 1) oz_gemm_kernel(const GArgs a) {
                      (warp >> 2) * (TN / 2) + TN / 2);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     __syncthreads();
-    epilogue_rows(a, tile, b, m0, nr0 / 2, tid, THREADS);
+    epilogue_rows<S>(a, tile, b, m0, nr0 / 2, tid, THREADS);
     if (!a.C2.null()) {
       __syncthreads();
-      epilogue_c2(a, tile, b, m0, nr0 / 2, tid, THREADS);
+      epilogue_c2<S>(a, tile, b, m0, nr0 / 2, tid, THREADS);
     }
   } else if (tid == 0) {
     atomicExch(&g_oz_error, 1);
@@ -829,7 +851,7 @@ int run_split(const MatRef& X, int rows, int K, int conj, bool isb, bool strided
     QTX_CHECK_LAUNCH();
     return QTX_OK;
   }
-  dim3 grid(rows_p / SPLIT_ROWS, (unsigned)bc);
+  dim3 grid((rows_p + SPLIT_ROWS - 1) / SPLIT_ROWS, (unsigned)bc);
   auto launch = [&](auto kern) -> int {
     QTX_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SPLIT_SMEM));
     kern<<<grid, THREADS, SPLIT_SMEM, s>>>(a);
@@ -850,7 +872,8 @@ int run_split(const MatRef& X, int rows, int K, int conj, bool isb, bool strided
 template <int S>
 int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
   using C = Cfg<S>;
-  const Geom g = geom(d.M, d.N, d.K);
+  static_assert(C::TNC == tnc_for(S), "padding unit of op(B) matches the tile");
+  const Geom g = geom(d.M, d.N, d.K, C::TNC);
   const bool bca = d.A.stride == 0, bcb = d.B.stride == 0;
   const size_t a_item = sizeof(int) * (size_t)g.Mp + (size_t)S * g.Mp * g.Kp;
   const size_t b_item = sizeof(int) * (size_t)g.Np + (size_t)S * 2 * g.Np * g.Kp;
@@ -862,7 +885,7 @@ int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
     set_error("zgemm (int8 emulation): scratch too small for one batch entry");
     return QTX_ERR_WORKSPACE;
   }
-  const size_t smem = (size_t)C::NS * C::STAGE + 1024 + 256 + sizeof(int) * (TM + TNC);
+  const size_t smem = (size_t)C::NS * C::STAGE + 1024 + 256 + sizeof(int) * (TM + C::TNC);
   QTX_CHECK_CUDA(cudaFuncSetAttribute(oz_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int64_t b0 = 0; b0 < d.batch; b0 += bc) {
     const int64_t n = std::min<int64_t>(bc, d.batch - b0);
@@ -904,7 +927,7 @@ int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
     a.scale3 = d.scale3;
     a.active = d.active;
     ProfScope prof(QTX_KERNEL_ZGEMM_EMU, 8.0 * d.M * d.N * (double)d.K * (double)n, s);
-    dim3 grid(2 * g.Np / TN, g.Mp / TM, (unsigned)n);
+    dim3 grid(2 * g.Np / C::TN, g.Mp / TM, (unsigned)n);
     oz_gemm_kernel<S><<<grid, THREADS, smem, s>>>(a);
     QTX_CHECK_LAUNCH();
   }
@@ -915,7 +938,7 @@ int run(const GemmDesc& d, void* scratch, size_t bytes, cudaStream_t s) {
 
 size_t oz_scratch_bytes(int M, int N, int K, int64_t batch, int slices) {
   if (slices <= 0 || batch <= 0) return 0;
-  const Geom g = geom(M, N, K);
+  const Geom g = geom(M, N, K, tnc_for(slices));
   return g.item_bytes(slices) * (size_t)std::min<int64_t>(batch, 65535) + 1024;
 }
 

@@ -46,14 +46,15 @@ def _check(got, a, b, op_a, op_b, slices, extra=0.0):
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (2, 3, 5), (17, 33, 9), (64, 64, 64), (100, 70, 130),
                                    (256, 256, 256), (65, 129, 257), (128, 32, 512)])
 @pytest.mark.parametrize("op_a,op_b", [(0, 0), (0, 1), (1, 0), (1, 1)])
-def test_emulated_zgemm_matches_numpy(cuda_device, m, n, k, op_a, op_b):
+@pytest.mark.parametrize("slices", [5, 6])  # 48- and 64-column tiles
+def test_emulated_zgemm_matches_numpy(cuda_device, m, n, k, op_a, op_b, slices):
     rng = np.random.default_rng(7 * m + 3 * n + k + 11 * op_a + 5 * op_b)
     B = 3
     a = _rand(rng, B, *((k, m) if op_a else (m, k)))
     b = _rand(rng, B, *((n, k) if op_b else (k, n)))
     C = zgemm_emulated(torch.from_numpy(a).to(cuda_device), torch.from_numpy(b).to(cuda_device),
-                       op_a=op_a, op_b=op_b, slices=6)
-    _check(C.cpu().numpy(), a, b, op_a, op_b, 6)
+                       op_a=op_a, op_b=op_b, slices=slices)
+    _check(C.cpu().numpy(), a, b, op_a, op_b, slices)
     assert status() == 0
 
 
