@@ -1002,6 +1002,22 @@ def run_kernels(args, local):
         del wsS
     out["zgemm_emulated_int8"] = emu
     del ref
+    # The same at 512x512 blocks, batch 74 (twice the K per output tile).
+    n2, B2 = 512, min(74, B)
+    flops2 = 8.0 * n2 ** 3 * B2
+    a2 = torch.randn((B2, n2, n2), dtype=torch.complex128, device=device, generator=g)
+    b2 = torch.randn((B2, n2, n2), dtype=torch.complex128, device=device, generator=g)
+    c2 = torch.empty_like(a2)
+    t_d = timeit(lambda: _native.check(lib.qtx_zgemm_batched(n2, n2, n2, B2, 1.0, 0.0, mat(a2), 0, mat(b2), 0, 0.0,
+                                                             0.0, z, 0, mat(c2), stream())))
+    emu2 = {"zgemm_ours_tflops": flops2 / t_d / 1e12}
+    for S in (5, 6, 7):
+        wsS = torch.empty(workspace_bytes(n2, n2, n2, B2, S), dtype=torch.uint8, device=device)
+        t = timeit(lambda: zgemm_emulated(a2, b2, slices=S, out=c2, workspace=wsS))
+        emu2[f"slices_{S}"] = {"fp64_equivalent_tflops": flops2 / t / 1e12, "speedup_vs_zgemm_ours": t_d / t}
+        del wsS
+    out["zgemm_emulated_int8_512_b74"] = emu2
+    del a2, b2, c2
     eye = torch.eye(n, dtype=torch.complex128, device=device)
     w = (a + n * eye).contiguous()  # well conditioned
     info = torch.zeros(B, dtype=torch.int32, device=device)
