@@ -57,7 +57,7 @@ constexpr int KS = 64;                 // int8 K per pipeline stage (64-byte row
 constexpr int THREADS = 256;
 constexpr int PLANE_A = TM * KS;       // 8 KB
 constexpr int SPLIT_ROWS = 32;         // op-rows per split CTA
-constexpr int SPLIT_K = 64;            // complex k per split tile
+constexpr int SPLIT_K = 32;            // complex k per split tile (4 per thread)
 constexpr long long kWaitLimit = 1ll << 26;
 
 __device__ int g_oz_error = 0;
@@ -224,7 +224,7 @@ constexpr int SPLIT_TILE = SPLIT_ROWS * SPLIT_LD;                // complex elem
 constexpr size_t SPLIT_SMEM = 2 * SPLIT_TILE * sizeof(double2);  // two tiles (double buffer)
 
 template <int S, bool ISB, bool STRIDED>
-__global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a) {
+__global__ void __launch_bounds__(THREADS, 4) oz_split_kernel(const SplitArgs a) {
   constexpr int L = 8 * S - 2;
   extern __shared__ __align__(16) uint8_t split_smem[];
   double2* tiles = reinterpret_cast<double2*>(split_smem);  // [2][SPLIT_ROWS][SPLIT_LD]
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
   const double sgn = a.conj ? -1.0 : 1.0;
 
   // K tile t of the strip -> shared buffer `buf` (cp.async, zero-filled
-  // outside the matrix); column perm(k) = 8 (k % 8) + k / 8 within a row.
+  // outside the matrix); column perm(k) = 8 (k % 4) + k / 4 within a row.
   auto load_tile = [&](int t, int buf) {
     double2* tl = tiles + buf * SPLIT_TILE;
     const int k0 = t * SPLIT_K;
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
       for (int i = warp; i < SPLIT_K; i += 8) {
         const int k = k0 + i, r = r0 + lane;
         const bool ok = k < a.K && r < a.rows;
-        cp_async16z(smem_addr(tl + lane * SPLIT_LD + 8 * (i & 7) + (i >> 3)),
+        cp_async16z(smem_addr(tl + lane * SPLIT_LD + 8 * (i & 3) + (i >> 2)),
                     ok ? X + (int64_t)k * a.X.ld + r : X, ok);
       }
     } else {
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
         for (int j = lane; j < SPLIT_K; j += 32) {
           const int k = k0 + j;
           const bool ok = k < a.K && r < a.rows;
-          cp_async16z(smem_addr(tl + i * SPLIT_LD + 8 * (j & 7) + (j >> 3)), ok ? X + (int64_t)r * a.X.ld + k : X,
+          cp_async16z(smem_addr(tl + i * SPLIT_LD + 8 * (j & 3) + (j >> 2)), ok ? X + (int64_t)r * a.X.ld + k : X,
                       ok);
         }
       }
@@ -331,10 +331,10 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
   if (tid < SPLIT_ROWS && r0 + tid < a.rows_p) a.expo[(int64_t)bl * a.rows_p + r0 + tid] = rexp[tid];
 
   // Sweep 2: digits, SPLIT_K complex k at a time through shared memory. The
-  // tile stores k at column perm(k) = 8 (k % 8) + k / 8, so the 8 lanes that
-  // read 8 consecutive k each hit distinct banks.
+  // tile stores k at column perm(k) = 8 (k % 4) + k / 4, so the 8 lanes that
+  // read 4 consecutive k each hit distinct banks.
   const int rr = tid >> 3;       // op-row of this thread
-  const int kc = (tid & 7) * 8;  // first of its 8 k in the tile
+  const int kc = (tid & 7) * 4;  // first of its 4 k in the tile
   const int e = scale_exp(rexp[rr]);
   const int sx = L - e;  // x 2^sx is the integer X before rounding
   const bool fast = sx >= -1000 && sx <= 1000;
@@ -363,10 +363,10 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
     // significant first) is byte S-1-p. -X_im gets its own Z (its digits are
     // not the negated digits of X_im where one is -128).
     constexpr unsigned long long kC = 0x8080808080808080ull >> (8 * (8 - S));
-    uint32_t zr[8][2], zi[8][2], zn[8][2];
+    uint32_t zr[4][2], zi[4][2], zn[4][2];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const double2 v = tl[rr * SPLIT_LD + 8 * j + (kc >> 3)];  // k = kc + j
+    for (int j = 0; j < 4; ++j) {
+      const double2 v = tl[rr * SPLIT_LD + 8 * j + (kc >> 2)];  // k = kc + j
       const long long xr = __double2ll_rn(fast ? v.x * fx : scalbn(v.x, sx));
       const long long xi = __double2ll_rn(fast ? sgn * v.y * fx : scalbn(sgn * v.y, sx));
       const unsigned long long ur = ((unsigned long long)xr + kC) ^ kC;
@@ -385,9 +385,9 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
       const int hw = bi >> 2;            // its 32-bit half
       const uint32_t sel = (uint32_t)(bi & 3);
       const uint32_t pair = sel | ((4u + sel) << 4);  // byte sel of x, byte sel of y
-      uint32_t w0[4], w1[4];
+      uint32_t w0[2], w1[2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < 2; ++q) {
         const int j0 = 2 * q, j1 = 2 * q + 1;
         if (ISB) {
           // row 2j: (re, -im); row 2j+1: (im, re)
@@ -401,21 +401,23 @@ __global__ void __launch_bounds__(THREADS, 3) oz_split_kernel(const SplitArgs a)
           w1[q] = 0u;
         }
       }
-      // plane block (p, entry, row tile, K block) as the GEMM stages load it
-      const int col = 2 * kb;  // byte column: one 16-byte swizzle chunk
-      const size_t kblk = (size_t)(col / KS), ch = (size_t)((col % KS) / 16);
+      // plane block (p, entry, row tile, K block) as the GEMM stages load it:
+      // 8 bytes = one half of a 16-byte swizzle chunk
+      const int col = 2 * kb;  // byte column
+      const size_t kblk = (size_t)(col / KS);
+      const int ch = (col % KS) / 16, half = col & 15;
       int8_t* ptile = a.planes + (size_t)p * plane + (size_t)bl * prows * a.Kp;
-      const uint4 v0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+      const uint2 v0 = make_uint2(w0[0], w0[1]);
       if (ISB) {
-        const uint4 v1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+        const uint2 v1 = make_uint2(w1[0], w1[1]);
         const int r2 = 2 * row;
         constexpr int TNB = Cfg<S>::TN;
         int8_t* blk = ptile + ((size_t)(r2 / TNB) * nkb + kblk) * Cfg<S>::PLANE_B;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB, (int)ch)) = v0;
-        *reinterpret_cast<uint4*>(blk + swz_offset(r2 % TNB + 1, (int)ch)) = v1;
+        *reinterpret_cast<uint2*>(blk + swz_offset(r2 % TNB, ch) + half) = v0;
+        *reinterpret_cast<uint2*>(blk + swz_offset(r2 % TNB + 1, ch) + half) = v1;
       } else {
         int8_t* blk = ptile + ((size_t)(row / TM) * nkb + kblk) * PLANE_A;
-        *reinterpret_cast<uint4*>(blk + swz_offset(row % TM, (int)ch)) = v0;
+        *reinterpret_cast<uint2*>(blk + swz_offset(row % TM, ch) + half) = v0;
       }
     }
     __syncthreads();  // buffer t & 1 is refilled at iteration t + 1
