@@ -21,7 +21,7 @@ def _copy(r):
     return r.transmission.copy(), r.density.copy(), r.current.copy()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "emulated"])
 def test_alone_equals_mixed_traffic(cuda_device, precision):
     cat = _catalogue()
     probe = np.array([1, 4, 5, 9, 13, 20, 22])
