@@ -28,5 +28,7 @@ def test_bench_arguments_parse():
     out = subprocess.run([sys.executable, "bench.py", "--help"], cwd=ROOT, capture_output=True, text=True,
                          timeout=120)
     assert out.returncode == 0
-    for flag in ("--gpus", "--steps", "--warmup", "--impl", "--workload", "--precision", "--graph"):
+    for flag in ("--gpus", "--steps", "--warmup", "--impl", "--workload", "--precision", "--graph",
+                 "--emulated-slices"):
         assert flag in out.stdout
+    assert "emulated" in out.stdout  # a --precision choice
