@@ -351,6 +351,49 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
                     f"stacks, {B} energies per step (RGF max_batch_size {min(sub, B)}), {steps} steps"}
 
 
+def host_link(torch, device, nbytes=1 << 30, reps=5) -> dict:
+    """Pinned host <-> device copy bandwidth on this GPU: H2D alone, D2H alone
+    and both directions at once on two streams (GB/s, best of `reps`, CUDA
+    events). The roofline of the end-to-end leg, whose every step uploads its
+    inputs and downloads its results."""
+    h_src = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    h_dst = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d_a = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    d_b = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    s1, s2 = torch.cuda.Stream(device), torch.cuda.Stream(device)
+
+    def timed(fn):
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            fn()
+            ev1.record()
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            best = ms if best is None else min(best, ms)
+        return best * 1e-3
+
+    def duplex():
+        cur = torch.cuda.current_stream(device)
+        s1.wait_stream(cur)
+        s2.wait_stream(cur)
+        with torch.cuda.stream(s1):
+            d_a.copy_(h_src, non_blocking=True)
+        with torch.cuda.stream(s2):
+            h_dst.copy_(d_b, non_blocking=True)
+        cur.wait_stream(s1)
+        cur.wait_stream(s2)
+
+    h2d = nbytes / timed(lambda: d_a.copy_(h_src, non_blocking=True)) / 1e9
+    d2h = nbytes / timed(lambda: h_dst.copy_(d_b, non_blocking=True)) / 1e9
+    dup = 2 * nbytes / timed(duplex) / 1e9
+    del h_src, h_dst, d_a, d_b
+    return {"h2d_gbs": h2d, "d2h_gbs": d2h, "duplex_gbs": dup, "bytes_per_copy": nbytes,
+            "how": f"pinned host <-> device copies of {nbytes >> 20} MiB, best of {reps}, CUDA events"}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import torch.distributed as dist
@@ -562,6 +605,13 @@ def run_ours(args, world, rank, local):
             e2e["h2d_bytes_per_step"] = int(agg[1].item())
             e2e["d2h_bytes_per_step"] = int(agg[2].item())
             e2e["path"] += f"; {world} ranks, {pick.size} energies per rank, max time over ranks"
+        link = host_link(torch, device)
+        secs = e2e["seconds"] if world == 1 else float(tmax.item())
+        moved = (e2e["h2d_bytes_per_step"] + e2e["d2h_bytes_per_step"]) * args.e2e_steps / secs / 1e9
+        e2e["link_gbs"] = link["duplex_gbs"] * world
+        e2e["link_frac"] = moved / e2e["link_gbs"]
+        e2e["link"] = dict(link, achieved_gbs=moved, note="achieved = (h2d + d2h bytes per step) x steps / "
+                           "time; link_gbs = simultaneous H2D + D2H bandwidth x ranks")
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.cpu_energies)
     if world > 1:
@@ -577,7 +627,11 @@ def run_ours(args, world, rank, local):
                     "frac": (achieved / peak["peak"]) if achieved and peak["peak"] else None,
                     "peak_source": "measured cuBLAS FP64 (max of DGEMM 8192^3, ZGEMM 4096^3) on this GPU; "
                                    "no FP64 entry in MEASURED_PEAKS.json",
-                    "peak_detail": peak, "traffic": _ncu_traffic(), "launches": gemm_n}
+                    "peak_detail": peak, "traffic": _ncu_traffic(),
+                    "traffic_source": "stored ncu capture of one full-batch launch "
+                                      "(profiles/zgemm_traffic.txt: dram__bytes_read.sum + dram__bytes_write.sum), "
+                                      "not measured in this run",
+                    "launches": gemm_n}
     elif main_prec == "emulated":
         S = args.emulated_slices
         tops = achieved * (S * (S + 1) // 2) if achieved else None  # int8 ops = 8mnk x digit pairs

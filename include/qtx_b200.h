@@ -54,13 +54,6 @@ enum qtx_status {
 
 enum qtx_dtype { QTX_C128 = 0, QTX_C64 = 1 };
 
-/* Precision of the arithmetic. QTX_FP64: complex128 throughout (FP64
- * tensor-core MMA). QTX_MIXED: complex64 storage, tensor-core products in
- * split-BF16 with FP32 accumulation, Newton-Schulz-refined inverses; FP64
- * only for the pivoted LU of the Schur-complement blocks and for the
- * Sancho-Rubio convergence test. */
-enum qtx_precision { QTX_FP64 = 0, QTX_MIXED = 1 };
-
 typedef struct qtx_mat {
   void* ptr;      /* device pointer to element (0, 0) of stack entry 0 */
   int64_t ld;     /* row stride, complex elements */
@@ -168,10 +161,13 @@ int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt*
  * every GPU that loads it until exit). For callers that cannot call
  * cudaMalloc/cudaFree during a solve (both synchronise the device and fail
  * once another allocator owns the memory). Requests needing more than 64 MiB
- * (sum_i b_i^2 + 6 b_max^2 complex128 per energy) return QTX_ERR_WORKSPACE.
- * All calls share the array: calls that overlap on the GPU race. A device's
- * first call resolves the array's device address; make it before any stream
- * capture. This entry point has no counterpart in the reference. */
+ * (sum_i b_i^2 + 6 b_max^2 complex128 per energy) return QTX_ERR_WORKSPACE
+ * before anything is enqueued or written. All calls share the array: calls
+ * that overlap on the GPU race. A device's first call resolves the array's
+ * device address; make it before any stream capture. It always runs the FP64
+ * DMMA products and the one-CTA-per-block inverse: the thread's GEMM path
+ * (qtx_set_gemm_path) and qtx_set_inverse_path do not apply to it. This entry
+ * point has no counterpart in the reference. */
 int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x,
                             int64_t batch, int* info, qtx_stream stream);
 
@@ -204,11 +200,14 @@ int qtx_selected_solve(const qtx_bt* a, const qtx_bt* sigma_lesser, const qtx_bt
 size_t qtx_selected_solve_mixed_workspace(int32_t num_blocks, const int32_t* block_sizes,
                                           int64_t batch, int return_current);
 
-/* qtx_selected_solve in mixed precision (QTX_MIXED): all block stacks are
+/* qtx_selected_solve in mixed precision: all block stacks are
  * complex64; block products run on the tcgen05 tensor cores as split-TF32
  * products with FP32 accumulation; every Schur-complement block is inverted
- * in FP64 (upcast, Gauss-Jordan with partial pivoting, rounded back). The
- * current and the density are accumulated in double. g0n is complex64. */
+ * in FP64 (upcast, Gauss-Jordan with partial pivoting, rounded back once,
+ * so no Newton-Schulz refinement step is applied). The current and the
+ * density are accumulated in double. g0n is complex64. The boundary
+ * conditions (qtx_sancho_rubio*, qtx_obc_refine, qtx_contact_self_energy)
+ * stay complex128 calls. */
 int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
                              const qtx_bt* sigma_greater, const qtx_mat* obc_retarded,
                              const qtx_mat* obc_lesser, const qtx_mat* obc_greater, const qtx_bt* xl,

@@ -26,6 +26,10 @@
 //    that first call on each device before any stream capture begins.
 //  * With the launch profiler off (the default) the call performs no device
 //    or host allocation.
+//  * Arithmetic: always the FP64 DMMA products and the one-CTA-per-block
+//    Gauss-Jordan inverse. The calling thread's GEMM path (qtx_set_gemm_path)
+//    and the inverse-path knob are ignored: the int8-emulated products and
+//    the multi-CTA inverse need scratch that is not part of the array.
 #include <mutex>
 
 #include "common.cuh"
@@ -109,6 +113,17 @@ void plus(GemmDesc& d, const MatRef& m, z64 coef) {
   if (!m.null()) d.add[d.nadd++] = Addend{m, coef, 0};
 }
 
+// Selects the FP64 DMMA products for the scope and restores the calling
+// thread's GEMM path afterwards.
+struct Fp64Products {
+  int prev;
+  Fp64Products() : prev(gemm_slices()) { set_gemm_slices(0); }
+  ~Fp64Products() { set_gemm_slices(prev); }
+};
+
+int selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x,
+                        int64_t batch, int* info, cudaStream_t s);
+
 }  // namespace
 }  // namespace qtx
 
@@ -117,6 +132,24 @@ using namespace qtx;
 extern "C" int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded,
                                        const qtx_bt* x, int64_t batch, int* info,
                                        qtx_stream stream) {
+  // No C++ exception may cross the C ABI.
+  try {
+    Fp64Products fp64;
+    return selected_inv_static(a, obc_retarded, x, batch, info, (cudaStream_t)stream);
+  } catch (const std::exception& e) {
+    set_error(std::string("qtx_selected_inv_static: internal error: ") + e.what());
+    return QTX_ERR_ARG;
+  } catch (...) {
+    set_error("qtx_selected_inv_static: internal error");
+    return QTX_ERR_ARG;
+  }
+}
+
+namespace qtx {
+namespace {
+
+int selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x,
+                        int64_t batch, int* info, cudaStream_t s) {
   if (a == nullptr || x == nullptr || batch <= 0 || a->num_blocks <= 0 ||
       a->block_sizes == nullptr || a->diag == nullptr || x->num_blocks != a->num_blocks ||
       x->block_sizes == nullptr || x->diag == nullptr ||
@@ -146,7 +179,6 @@ extern "C" int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retar
   void* base = nullptr;
   QTX_TRY(scratch_address(&base));
   L.base = static_cast<char*>(base);
-  cudaStream_t s = (cudaStream_t)stream;
   if (info) QTX_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
   const z64 one{1.0, 0.0}, mone{-1.0, 0.0};
   auto obc = [&](int i) { return obc_retarded ? mref(obc_retarded[i]) : MatRef{}; };
@@ -196,3 +228,6 @@ extern "C" int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retar
   }
   return QTX_OK;
 }
+
+}  // namespace
+}  // namespace qtx

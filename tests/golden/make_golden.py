@@ -1,9 +1,9 @@
 """Generates the golden fixtures in this directory from the reference package.
 
-Run in a checkout that has the quatrex reference sources (Python, NumPy
-backend) at ``$QTX_REFERENCE_SRC`` (default ``/root/reference/src``)::
+Run with the quatrex reference sources (Python, NumPy backend) at
+``$QTX_REFERENCE_SRC`` (the reference's ``src/`` directory, required)::
 
-    python tests/golden/make_golden.py
+    QTX_REFERENCE_SRC=<quatrex checkout>/src python tests/golden/make_golden.py
 
 The reference needs ``mpi4py`` and ``h5py`` at import time; neither is on the
 solver path, so the single-rank stand-ins under ``_stubs/`` are put first on
@@ -30,9 +30,11 @@ import time
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+if "QTX_REFERENCE_SRC" not in os.environ:
+    sys.exit("set QTX_REFERENCE_SRC to the reference's src/ directory (it holds qttools/ and quatrex/)")
 os.environ["QTX_ARRAY_MODULE"] = "numpy"
 sys.path.insert(0, str(HERE / "_stubs"))
-sys.path.insert(0, os.environ.get("QTX_REFERENCE_SRC", "/root/reference/src"))
+sys.path.insert(0, os.environ["QTX_REFERENCE_SRC"])
 sys.path.insert(0, str(HERE.parent.parent))
 
 import numpy as np  # noqa: E402

@@ -6,8 +6,11 @@ the GPU's memory a fresh allocation fails or fragments it. This entry point
 takes its scratch from a 64 MiB device array inside the library instead of a
 caller workspace. The test calls it through the C ABI twice in a row (the
 array keeps the previous call's contents) and compares each result with
-the workspace-based qtx_selected_inv at the FP64 tolerance of the RGF tests,
-then checks that an oversize request is refused before any work is done.
+the workspace-based qtx_selected_inv at the FP64 tolerance of the RGF tests
+and, once, with the CPU oracle's selected inversion; it checks that the entry
+point keeps to the FP64 products when the calling thread selected the
+int8-emulated GEMM path, and that an oversize request is refused with
+nothing enqueued or written.
 This file is collected last so that a stop at the first failure has run every
 other test already; it also passes when run alone.
 """
@@ -18,6 +21,7 @@ import numpy as np
 import pytest
 import torch
 
+from oracle import negf_oracle as o
 from quatrex_b200 import _native
 from quatrex_b200._interop import mat
 from quatrex_b200._native import NULL_MAT, QtxBT, QtxMat
@@ -106,15 +110,60 @@ def test_static_scratch_matches_workspace_version_twice(cuda_device):
         assert _rel(g, r) < RTOL
 
 
+def test_static_scratch_matches_oracle(cuda_device):
+    """Diagonal and off-diagonal blocks of (A - OBC)^{-1} against the oracle's
+    restatement of rgf.py:25-113 on the same blocks."""
+    lib = _native.load()
+    block_sizes, batch = [48, 64, 17, 64, 32], 3
+    prob = _problem(block_sizes, batch, cuda_device, 4)
+    got = _solve(lib, block_sizes, batch, prob, static=True, device=cuda_device)
+    diag, upper, lower, obc = ([None if t is None else t.cpu().numpy() for t in x] for x in prob)
+    xd, xu, xl = o.selected_inv(diag, upper, lower, obc)
+    n = len(block_sizes)
+    refs = list(xd) + list(xu) + list(xl)
+    assert len(got) == len(refs) == 3 * n - 2
+    for g, r in zip(got, refs):
+        assert _rel(g, r) < 1e-10
+
+
+def test_static_scratch_ignores_emulated_gemm_path(cuda_device):
+    """With the int8-emulated products selected on the calling thread, the
+    entry point still runs the FP64 products (its array holds no digit
+    planes) and leaves the thread's selection as it was."""
+    lib = _native.load()
+    block_sizes, batch = [64] * 6, 4
+    prob = _problem(block_sizes, batch, cuda_device, 9)
+    fp64 = _solve(lib, block_sizes, batch, prob, static=False, device=cuda_device)
+    _native.check(lib.qtx_set_gemm_path(5))
+    try:
+        got = _solve(lib, block_sizes, batch, prob, static=True, device=cuda_device)
+        assert lib.qtx_get_gemm_path() == 5
+        emulated = _solve(lib, block_sizes, batch, prob, static=False, device=cuda_device)
+    finally:
+        _native.check(lib.qtx_set_gemm_path(0))
+    for g, r in zip(got, fp64):
+        assert _rel(g, r) < RTOL
+    # the workspace path did switch to the emulated products (differs at ~1e-10)
+    assert max(_rel(e, r) for e, r in zip(emulated, fp64)) > 0.0
+
+
 def test_static_scratch_rejects_oversize(cuda_device):
     lib = _native.load()
     keep = []
-    big = torch.empty((1, 1), dtype=torch.complex128, device=cuda_device)
-    n = 4
-    bs = (ctypes.c_int32 * n)(*([1024] * n))
-    m = (QtxMat * n)(*([QtxMat(big.data_ptr(), 1024, 0)] * n))
-    a = QtxBT(n, bs, m, m, m)
-    keep.append((bs, m))
-    st = lib.qtx_selected_inv_static(ctypes.byref(a), None, ctypes.byref(a), 4, None, _stream())
+    n, b, batch = 4, 1024, 4
+    inp = torch.ones((batch, b, b), dtype=torch.complex128, device=cuda_device)
+    out = torch.full((batch, b, b), 7.0 + 3.0j, dtype=torch.complex128, device=cuda_device)
+    bs = (ctypes.c_int32 * n)(*([b] * n))
+    m_in = (QtxMat * n)(*([mat(inp)] * n))
+    m_out = (QtxMat * n)(*([mat(out)] * n))
+    a = QtxBT(n, bs, m_in, m_in, m_in)
+    x = QtxBT(n, bs, m_out, m_out, m_out)
+    keep.append((bs, m_in, m_out))
+    info = torch.full((batch,), -77, dtype=torch.int32, device=cuda_device)
+    st = lib.qtx_selected_inv_static(ctypes.byref(a), None, ctypes.byref(x), batch, info.data_ptr(), _stream())
+    torch.cuda.synchronize()
     assert st == _native.QTX_ERR_WORKSPACE
     assert b"static scratch" in lib.qtx_last_error()
+    # refused before anything was enqueued: outputs and info keep their sentinels
+    assert bool((out == 7.0 + 3.0j).all())
+    assert bool((info == -77).all())
