@@ -332,18 +332,25 @@ def e2e_leg(torch, device, dev, energies, steps, sub=8):
         phase["density"] += t3 - t2
         return cur, dens
 
+    from quatrex_b200 import _interop
+
     step()  # warm-up
     torch.cuda.synchronize()
     for k in phase:
         phase[k] = 0.0
+    _interop.transfer_bytes.update(h2d=0, d2h=0)
     t0 = time.perf_counter()
     for _ in range(steps):
         cur, dens = step()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    elem = 16
-    h2d = 3 * B * proto.nnz * elem + 6 * B * b * b * elem  # A, Sigma^<, Sigma^> + contact blocks
-    d2h = 3 * B * proto.nnz * elem + B * (n + 1) * elem + 6 * B * b * b * elem
+    # bytes the plugin moved between the host containers and the GPU (counted
+    # from the tensors it copied): A in full, the diagonal and upper blocks of
+    # Sigma^< / Sigma^> (the only ones the solve reads), the contact blocks,
+    # X^< / X^> in full, the diagonal blocks of X^R, surface Green's functions,
+    # self-energies, current and density
+    h2d = _interop.transfer_bytes["h2d"] / steps
+    d2h = _interop.transfer_bytes["d2h"] / steps
     return {"value": steps * B / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "energies": steps * B, "seconds": dt,
             "seconds_per_step": {k: v / steps for k, v in phase.items()},

@@ -309,6 +309,17 @@ int qtx_coo_densify(int64_t batch, const void* data, int64_t data_stride, int64_
 int qtx_coo_sparsify(int64_t batch, qtx_mat in, int64_t nnz, const int32_t* rows,
                      const int32_t* cols, void* data, int64_t data_stride, qtx_stream stream);
 
+/* Copies the byte ranges [offsets[r], offsets[r] + lengths[r]) of each of
+ * `rows` rows from src (row pitch src_row_bytes) to dst (row pitch
+ * dst_row_bytes), host or device memory in any direction (a pinned host
+ * buffer makes it an asynchronous DMA); offsets / lengths are host arrays.
+ * The plugin layer moves only the nonzero slices of the DSDBCOO blocks a
+ * solve reads or writes (dsdbcoo.py:297-331) with it; replaces the
+ * reference's per-block host views of data[stack, nnz]. */
+int qtx_copy_ranges(void* dst, int64_t dst_row_bytes, const void* src, int64_t src_row_bytes,
+                    int64_t rows, const int64_t* offsets, const int64_t* lengths, int num_ranges,
+                    qtx_stream stream);
+
 /* Complex energies z[b] = E[b] + i eta (device double[batch] in, device
  * complex128[batch] out), the scalar part of the system-matrix assembly. */
 int qtx_assemble_energies(int64_t batch, const double* energies, double eta, void* z,

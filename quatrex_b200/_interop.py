@@ -28,6 +28,14 @@ from ._native import NULL_MAT, QtxMat
 _C128 = torch.complex128
 _ELEM = 16  # bytes of one complex128
 
+# Bytes moved between host and device memory by this module (the plugin's
+# inputs, outputs and boundary blocks); read by the end-to-end benchmark.
+transfer_bytes = {"h2d": 0, "d2h": 0}
+
+
+def _count(direction: str, t) -> None:
+    transfer_bytes[direction] += int(t.numel()) * int(t.element_size())
+
 
 # ---------------------------------------------------------------------------
 # Arrays
@@ -55,11 +63,14 @@ def to_device(x, device: torch.device, dtype=_C128) -> torch.Tensor:
         t = x
         if t.device != device:
             t = t.to(device, non_blocking=True)
+            if x.device.type == "cpu":
+                _count("h2d", x)
     elif k == "cupy":
         t = torch.from_dlpack(x)
     else:
         arr = np.asarray(x)
         t = torch.from_numpy(np.ascontiguousarray(arr)).to(device, non_blocking=False)
+        _count("h2d", t)
     if t.dtype != dtype:
         t = t.to(dtype)
     return t
@@ -75,6 +86,7 @@ def from_device(t: torch.Tensor, like):
             # pinned host result: the copy is a DMA, and so is a later upload
             out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
             out.copy_(t, non_blocking=True)
+            _count("d2h", t)
             torch.cuda.current_stream(t.device).synchronize()
             return out
         return t.to(like.device)
@@ -82,6 +94,8 @@ def from_device(t: torch.Tensor, like):
         import cupy  # noqa: PLC0415 - only present when the caller uses CuPy
 
         return cupy.from_dlpack(t)
+    if t.is_cuda:
+        _count("d2h", t)
     return t.detach().cpu().numpy()
 
 
@@ -89,13 +103,51 @@ def assign(dst, src: torch.Tensor) -> None:
     """``dst[...] = src`` for a NumPy / CuPy / torch destination view."""
     k = kind(dst)
     if k == "torch":
+        if dst.device.type == "cpu" and src.is_cuda:
+            _count("d2h", src)
         dst.copy_(src.reshape(dst.shape))
     elif k == "cupy":
         import cupy  # noqa: PLC0415
 
         dst[...] = cupy.from_dlpack(src.contiguous()).reshape(dst.shape)
     else:
+        if src.is_cuda:
+            _count("d2h", src)
         dst[...] = src.detach().cpu().numpy().reshape(dst.shape)
+
+
+def merged_spans(entries) -> list[list[int]]:
+    """Sorted element ranges [start, stop) of the given block entries, with
+    touching ranges merged (block-sorted storage keeps (i, i) and (i, i+1)
+    adjacent)."""
+    spans: list[list[int]] = []
+    for a, b in sorted((e.start, e.stop) for e in entries):
+        if spans and spans[-1][1] == a:
+            spans[-1][1] = b
+        else:
+            spans.append([a, b])
+    return spans
+
+
+def copy_spans(dst: torch.Tensor, src: torch.Tensor, spans, stream) -> None:
+    """Copies the element ranges ``spans`` of every row of the (rows, nnz)
+    tensors src -> dst on ``stream`` (raw handle) with qtx_copy_ranges; one
+    of them may be host memory (pinned: an asynchronous DMA)."""
+    from ctypes import c_int64
+
+    if not spans:
+        return
+    esz = src.element_size()
+    rows = int(src.shape[0])
+    off = (c_int64 * len(spans))(*[a * esz for a, _ in spans])
+    ln = (c_int64 * len(spans))(*[(b - a) * esz for a, b in spans])
+    _native.check(_native.load().qtx_copy_ranges(dst.data_ptr(), dst.stride(0) * esz, src.data_ptr(),
+                                                 src.stride(0) * esz, rows, off, ln, len(spans), stream))
+    moved = rows * sum(b - a for a, b in spans) * esz
+    if src.device.type == "cpu" and dst.is_cuda:
+        transfer_bytes["h2d"] += moved
+    elif src.is_cuda and dst.device.type == "cpu":
+        transfer_bytes["d2h"] += moved
 
 
 def mat(t: torch.Tensor, offset_elems: int = 0, ld: int | None = None,
@@ -245,7 +297,15 @@ class BTView:
         # Inputs cross the bus as one contiguous copy (a DMA at full link
         # speed; per-block strided copies would be staged through pageable
         # memory).
-        if self.role == "in" or (k in ("torch", "cupy") and not host):
+        needed = [e for (i, j), e in self.layout.entries.items() if e is not None and (
+            "diag" if i == j else ("upper" if j == i + 1 else "lower")) in need]
+        partial = len(needed) < sum(e is not None for e in self.layout.entries.values())
+        if (self.role == "in" and host and k == "torch" and partial and src.is_contiguous()
+                and src.dtype == _C128 and src.numel()):
+            # only the blocks the solver reads cross the bus
+            t = torch.empty(src.shape, dtype=_C128, device=self.device)
+            copy_spans(t.reshape(-1, nnz), src.reshape(-1, nnz), merged_spans(needed), self.stream)
+        elif self.role == "in" or (k in ("torch", "cupy") and not host):
             t = to_device(src, self.device)
         else:
             # host output: nothing is uploaded; finalize() returns the written blocks
@@ -350,6 +410,13 @@ class BTView:
         src = self.data.reshape(self.data_src.shape)
         if len(written) == total:
             dst.copy_(src, non_blocking=True)
+            _count("d2h", src)
+            return None
+        if dst.is_contiguous() and dst.is_pinned():
+            # the written blocks go straight into the container (one DMA per span)
+            nnz = int(self.data.shape[-1])
+            copy_spans(dst.reshape(-1, nnz), self.data, merged_spans(written),
+                       torch.cuda.current_stream(self.device).cuda_stream)
             return None
         # Some blocks must keep the container's values: one contiguous DMA
         # into pinned staging now, the written ranges copied on the host by
@@ -385,13 +452,17 @@ class BTView:
                 if self._host and len(written) < total:
                     # only the blocks the solver wrote go back to the host container
                     dst = self.m.data[self.sl]
-                    hd = dst if kind(dst) == "torch" else None
-                    src = self.data.reshape(self.data_src.shape)
-                    for e in written:
-                        if hd is not None:
-                            hd[..., e.start:e.stop].copy_(src[..., e.start:e.stop], non_blocking=True)
-                        else:
+                    nnz = int(self.data.shape[-1])
+                    hd = dst if kind(dst) == "torch" else torch.from_numpy(dst) if (
+                        isinstance(dst, np.ndarray) and dst.dtype == np.complex128) else None
+                    if hd is not None and hd.is_contiguous():
+                        copy_spans(hd.reshape(-1, nnz), self.data, merged_spans(written),
+                                   torch.cuda.current_stream(self.device).cuda_stream)
+                    else:
+                        src = self.data.reshape(self.data_src.shape)
+                        for e in written:
                             dst[..., e.start:e.stop] = src[..., e.start:e.stop].cpu().numpy()
+                            transfer_bytes["d2h"] += int(src[..., e.start:e.stop].numel()) * _ELEM
                     torch.cuda.current_stream(self.device).synchronize()
                 else:
                     torch.cuda.current_stream(self.device).synchronize()

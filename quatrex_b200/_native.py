@@ -101,6 +101,8 @@ SIGNATURES = {
                                 c_int, c_void_p]),
     "qtx_coo_sparsify": (c_int, [c_int64, QtxMat, c_int64, c_void_p, c_void_p, c_void_p, c_int64,
                                  c_void_p]),
+    "qtx_copy_ranges": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int64, POINTER(c_int64),
+                                POINTER(c_int64), c_int, c_void_p]),
     "qtx_profile_enable": (c_int, [c_int]),
     "qtx_profile_reset": (c_int, []),
     "qtx_profile_read": (c_int, [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]),

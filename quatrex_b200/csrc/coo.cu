@@ -158,3 +158,35 @@ extern "C" int qtx_assemble_energies(int64_t batch, const double* energies, doub
   QTX_CHECK_LAUNCH();
   return QTX_OK;
 }
+
+// Copies the byte ranges [offsets[r], offsets[r] + lengths[r]) of every row
+// of a row-strided stack from src to dst (any direction; one 2D copy per
+// range on the stream). For a DSDBCOO data[stack, nnz] buffer the ranges
+// are the nonzero slices of the blocks one call reads or writes
+// (dsdbcoo.py:297-331): moving only those between host and device replaces
+// the reference's per-block host views (`stack[...]`, `.blocks[i, j]`).
+extern "C" int qtx_copy_ranges(void* dst, int64_t dst_row_bytes, const void* src,
+                               int64_t src_row_bytes, int64_t rows, const int64_t* offsets,
+                               const int64_t* lengths, int num_ranges, qtx_stream stream) {
+  if (rows <= 0 || num_ranges <= 0) return QTX_OK;
+  if (dst == nullptr || src == nullptr || offsets == nullptr || lengths == nullptr ||
+      dst_row_bytes <= 0 || src_row_bytes <= 0) {
+    set_error("qtx_copy_ranges: invalid arguments");
+    return QTX_ERR_ARG;
+  }
+  for (int r = 0; r < num_ranges; ++r) {
+    if (offsets[r] < 0 || lengths[r] < 0 || offsets[r] + lengths[r] > dst_row_bytes ||
+        offsets[r] + lengths[r] > src_row_bytes) {
+      set_error("qtx_copy_ranges: range " + std::to_string(r) + " outside the rows");
+      return QTX_ERR_ARG;
+    }
+  }
+  for (int r = 0; r < num_ranges; ++r) {
+    if (lengths[r] == 0) continue;
+    QTX_CHECK_CUDA(cudaMemcpy2DAsync(static_cast<char*>(dst) + offsets[r], (size_t)dst_row_bytes,
+                                     static_cast<const char*>(src) + offsets[r], (size_t)src_row_bytes,
+                                     (size_t)lengths[r], (size_t)rows, cudaMemcpyDefault,
+                                     (cudaStream_t)stream));
+  }
+  return QTX_OK;
+}

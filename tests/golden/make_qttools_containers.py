@@ -99,8 +99,11 @@ def main() -> None:
         record(out, name, x)
     # The reference's boundary current terms (rgf.py:414-428) use the whole
     # OBC stacks, so the current is taken with one batch covering the stack.
-    *_, current = RGF(max_batch_size=stack[0]).selected_solve(A, Bl, Bg, obc_blocks=obc, return_current=True)
-    out["current"] = np.asarray(current)
+    # (without out= the current is returned only together with X^R, rgf.py:430-435)
+    *_, current = RGF(max_batch_size=stack[0]).selected_solve(A, Bl, Bg, obc_blocks=obc, return_retarded=True,
+                                                              return_current=True)
+    assert isinstance(current, np.ndarray) and current.dtype == np.complex128
+    out["current"] = current
     x = RGF(max_batch_size=3).selected_inv(A, obc_blocks=obc)
     record(out, "inv", x)
     np.savez_compressed(HERE / "qttools_dsdbcoo.npz", **out)
