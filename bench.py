@@ -77,7 +77,7 @@ def parse():
                    help="arrival rate as a fraction of the capacity measured per lane")
     p.add_argument("--graph", action="store_true",
                    help="replay each batch through one captured CUDA graph (device-side Sancho-Rubio loop)")
-    p.add_argument("--inverse-path", choices=["auto", "single", "wide"], default="auto",
+    p.add_argument("--inverse-path", choices=["auto", "single", "wide", "cluster"], default="auto",
                    help="inverse kernels: automatic choice, one CTA per matrix, or multi-CTA panels")
     return p.parse_args()
 
@@ -1083,7 +1083,8 @@ def run_kernels(args, local):
     w = (a + n * eye).contiguous()  # well conditioned
     info = torch.zeros(B, dtype=torch.int32, device=device)
     ws = torch.empty(lib.qtx_zinv_workspace(n, B), dtype=torch.uint8, device=device)
-    for name, mode in (("zinv_ours_one_cta_per_matrix", 1), ("zinv_ours_multi_cta", 2)):
+    for name, mode in (("zinv_ours_one_cta_per_matrix", 1), ("zinv_ours_multi_cta", 2),
+                       ("zinv_ours_cluster", 3)):
         _native.check(lib.qtx_set_inverse_path(mode))
         out[name] = flops / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
             n, B, mat(w), mat(c), info.data_ptr(), ws.data_ptr(), ws.numel(), stream()))) / 1e12
@@ -1091,8 +1092,8 @@ def run_kernels(args, local):
     out["zinv_torch_linalg_inv"] = flops / timeit(lambda: torch.linalg.inv(w)) / 1e12
     # Inverse paths against the batch size (the automatic choice's crossover).
     sweep = {}
-    for nb in (8, 16, 32, 64, 96, 148):
-        for nn in (256, 384, 512):
+    for nb in (4, 8, 16, 32, 64, 96, 148, 296):
+        for nn in (128, 256, 384, 512):
             if nb > B:
                 continue
             wn = (torch.randn((nb, nn, nn), dtype=torch.complex128, device=device, generator=g)
@@ -1100,7 +1101,9 @@ def run_kernels(args, local):
             cn = torch.empty_like(wn)
             wsn = torch.empty(lib.qtx_zinv_workspace(nn, nb), dtype=torch.uint8, device=device)
             row = {}
-            for name, mode in (("one_cta", 1), ("multi_cta", 2)):
+            for name, mode in (("one_cta", 1), ("multi_cta", 2), ("cluster", 3)):
+                if mode == 3 and nn > 256:
+                    continue
                 _native.check(lib.qtx_set_inverse_path(mode))
                 row[name] = 8.0 * nn ** 3 * nb / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
                     nn, nb, mat(wn), mat(cn), info.data_ptr(), wsn.data_ptr(), wsn.numel(), stream()))) / 1e12
@@ -1123,7 +1126,7 @@ def main():
         return
     from quatrex_b200 import _native
 
-    _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2}[args.inverse_path]))
+    _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2, "cluster": 3}[args.inverse_path]))
     if args.workload != "cfg1":
         if rank == 0:
             {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels}[args.workload](args, local)

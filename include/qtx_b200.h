@@ -139,10 +139,18 @@ size_t qtx_zinv_workspace(int n, int64_t batch);
 int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, void* workspace,
                         size_t workspace_bytes, qtx_stream stream);
 
-/* Inverse path of every workspace-backed inverse in this process: 0
- * automatic (default), 1 one CTA per matrix, 2 multi-CTA. A tuning and test
- * knob; no reference counterpart. */
+/* Inverse path of every inverse in this process: 0 automatic (default),
+ * 1 one CTA per matrix, 2 multi-CTA (workspace-backed calls), 3 one
+ * thread-block cluster of ceil(n / 32) CTAs per matrix holding it in
+ * distributed shared memory (n <= 256; loaded with TMA). Automatic picks the
+ * cluster kernel for n <= 256 while the batch is at most four times the
+ * number of clusters the GPU holds at once. A tuning and test knob; no
+ * reference counterpart. */
 int qtx_set_inverse_path(int mode);
+/* 1 if a bounded wait inside the cluster inverse timed out since the last
+ * call (the flag is cleared; those results are invalid), 0 if not, < 0 on
+ * error. Synchronises the device. */
+int qtx_inverse_status(void);
 
 /* Workspace bytes for qtx_selected_inv on this block layout and batch. */
 size_t qtx_selected_inv_workspace(int32_t num_blocks, const int32_t* block_sizes, int64_t batch);

@@ -57,6 +57,7 @@ SIGNATURES = {
     "qtx_zinv_workspace": (c_size_t, [c_int, c_int64]),
     "qtx_zinv_batched_ws": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p, c_size_t, c_void_p]),
     "qtx_set_inverse_path": (c_int, [c_int]),
+    "qtx_inverse_status": (c_int, []),
     "qtx_zgemm_emulated_workspace": (c_size_t, [c_int, c_int, c_int, c_int64, c_int]),
     "qtx_zgemm_emulated_batched": (c_int, [c_int, c_int, c_int, c_int64, c_double, c_double, QtxMat, c_int,
                                            QtxMat, c_int, c_double, c_double, QtxMat, c_int, QtxMat, c_int,

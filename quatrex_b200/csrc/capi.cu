@@ -294,9 +294,15 @@ int qtx_emulated_gemm_status(void) {
   return st != QTX_OK ? st : flag;
 }
 
+int qtx_inverse_status(void) {
+  int flag = 0;
+  const int st = zinv_cluster_status_take(&flag);
+  return st != QTX_OK ? st : flag;
+}
+
 int qtx_set_inverse_path(int mode) {
-  if (mode < 0 || mode > 2) {
-    set_error("qtx_set_inverse_path: mode must be 0, 1 or 2");
+  if (mode < 0 || mode > 3) {
+    set_error("qtx_set_inverse_path: mode must be 0, 1, 2 or 3");
     return QTX_ERR_ARG;
   }
   set_inverse_path(mode);

@@ -158,6 +158,12 @@ int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* acti
             size_t scratch_bytes, cudaStream_t s);
 bool zinv_prefers_wide(int n, int64_t batch);
 void set_inverse_path(int mode);
+// One thread-block cluster of ceil(n / 32) CTAs per matrix with the matrix in
+// distributed shared memory (zinv_cluster.cu); n <= 256, no scratch.
+int zinv_cluster(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s);
+bool zinv_prefers_cluster(int n, int64_t batch);
+// Reads and clears the device flag of timed-out waits in zinv_cluster.
+int zinv_cluster_status_take(int* flag);
 
 // Elementwise combination (blockops.cu):
 //   out = sum_t coef_t * op_t(X_t)   for up to 4 terms, over an m x n stack.

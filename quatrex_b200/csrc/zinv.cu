@@ -692,6 +692,7 @@ int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active,
     set_error("zinv: null matrix");
     return QTX_ERR_ARG;
   }
+  if (zinv_prefers_cluster(n, batch)) return zinv_cluster(n, batch, A, X, info, active, s);
   if (n <= 400) return launch2<16>(n, batch, A, X, info, active, s);
   if (n <= 720) return launch2<8>(n, batch, A, X, info, active, s);
   if (n <= 1024) return launch<8>(n, batch, A, X, info, active, s);

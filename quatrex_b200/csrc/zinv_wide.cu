@@ -274,7 +274,7 @@ int run_wide(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* act
   return QTX_OK;
 }
 
-int g_inverse_path = 0;  // 0 automatic, 1 one CTA per matrix, 2 multi-CTA
+int g_inverse_path = 0;  // 0 automatic, 1 one CTA per matrix, 2 multi-CTA, 3 cluster
 
 int num_sms() {
   static int sms = 0;
@@ -300,8 +300,20 @@ size_t zinv_scratch_bytes(int n, int64_t batch) {
 
 void set_inverse_path(int mode) { g_inverse_path = mode; }
 
+bool zinv_prefers_cluster(int n, int64_t batch) {
+  if (n > 256) return false;
+  if (g_inverse_path == 3) return true;
+  if (g_inverse_path != 0) return false;
+  // A cluster per matrix (ceil(n / 32) CTAs, one per SM at n = 256) finishes
+  // one matrix far sooner than one CTA streaming it through HBM, but holds
+  // several SMs for it: it wins while the batch keeps few clusters waiting.
+  const int c = (n + 31) / 32;
+  const int resident = num_sms() / c;
+  return batch <= 4 * (int64_t)resident;
+}
+
 bool zinv_prefers_wide(int n, int64_t batch) {
-  if (g_inverse_path == 1) return false;
+  if (g_inverse_path == 1 || g_inverse_path == 3) return false;
   if (g_inverse_path == 2) return true;
   // One CTA per matrix leaves SMs idle when the batch is below the SM count;
   // the multi-CTA path pays n/NB launches and a pass over the matrix per
@@ -314,6 +326,7 @@ bool zinv_prefers_wide(int n, int64_t batch) {
 int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, void* scratch,
             size_t scratch_bytes, cudaStream_t s) {
   if (n <= 0 || batch <= 0) return QTX_OK;
+  if (zinv_prefers_cluster(n, batch)) return zinv_cluster(n, batch, A, X, info, active, s);
   if (scratch == nullptr || scratch_bytes < zinv_scratch_bytes(n, batch) || !zinv_prefers_wide(n, batch) ||
       n > 1024 || batch > 65535)
     return zinv(n, batch, A, X, info, active, s);
