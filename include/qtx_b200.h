@@ -143,9 +143,9 @@ int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, v
  * 1 one CTA per matrix, 2 multi-CTA (workspace-backed calls), 3 one
  * thread-block cluster of ceil(n / 32) CTAs per matrix holding it in
  * distributed shared memory (n <= 256; loaded with TMA). Automatic picks the
- * cluster kernel for n <= 256 while the batch is at most four times the
- * number of clusters the GPU holds at once. A tuning and test knob; no
- * reference counterpart. */
+ * cluster kernel for n <= 256 while batch x ceil(n / 32) is at most half the
+ * SM count (the small batches where one matrix's latency dominates). A
+ * tuning and test knob; no reference counterpart. */
 int qtx_set_inverse_path(int mode);
 /* 1 if a bounded wait inside the cluster inverse timed out since the last
  * call (the flag is cleared; those results are invalid), 0 if not, < 0 on

@@ -22,6 +22,7 @@
 //   Finally undo the column permutation (pivots applied in reverse order).
 // Total work n^3 complex multiply-adds = 8 n^3 real flops.
 #include "common.cuh"
+#include "gj_panel.cuh"
 
 namespace qtx {
 namespace {
@@ -411,7 +412,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
   int* aff_src = aff_row + 2 * NB;                       // 2 NB
   int* pivrow = aff_src + 2 * NB;                        // n
   int* colsrc = pivrow + n;                              // n
-  __shared__ int s_na;
+  __shared__ int s_na, s_sing;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
@@ -427,12 +428,25 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
         x[(int64_t)r * ldx + c] = a[(int64_t)r * A.ld + c];
       }
     }
-    int singular_at = 0;
+    if (tid == 0) s_sing = 0;
     __syncthreads();
 
     for (int k0 = 0; k0 < n; k0 += NB) {
       const int nbp = min(NB, n - k0);
-      // 1. Stage and factor the panel.
+      // 1. Stage the panel and factor it: in registers for 16-column panels
+      //    of at most 256 rows (two lanes per row), through shared memory
+      //    otherwise.
+      if (NB == 16 && n <= 256) {
+      for (int idx = tid; idx < n * NB; idx += T2) {
+        const int r = idx / NB, c = idx % NB;
+        P[r * PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+      gj_factor_panel16(
+          n, k0, nbp, [&](int r, int c) { return P[r * PS + c]; },
+          [&](int r, int c, z64 v) { P[r * PS + c] = v; }, pivrow, prow, rowk, red_v, red_i, &s_sing);
+      __syncthreads();
+      } else {
       for (int idx = tid; idx < n * NB; idx += T2) {
         const int r = idx / NB, c = idx % NB;
         P[r * PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
@@ -476,7 +490,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
           }
         }
         const int p = besti;
-        if (best <= 0.0 && singular_at == 0) singular_at = k + 1;
+        if (best <= 0.0 && tid == 0 && s_sing == 0) s_sing = k + 1;
         const z64 dpiv = zrecip(P[p * PS + kk]);
         if (tid < NB) {
           rowk[tid] = P[k * PS + tid];
@@ -511,6 +525,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
             }
           }
         }
+      }
       }
       // 2. The panel's interchanges as a permutation of the affected rows:
       //    row aff_row[a] receives the old content of row aff_src[a].
@@ -663,7 +678,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
         __syncwarp();
       }
     }
-    if (tid == 0 && info != nullptr && singular_at != 0 && info[b] == 0) info[b] = singular_at;
+    if (tid == 0 && info != nullptr && s_sing != 0 && info[b] == 0) info[b] = s_sing;
     __syncthreads();
   }
 }

@@ -41,6 +41,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "gj_panel.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -54,7 +55,6 @@ constexpr int CW = 32;          // columns per CTA
 constexpr int CNB = 16;         // panel width
 constexpr int CT = 512;         // threads per CTA
 constexpr int CWARPS = CT / 32;
-constexpr int TS = CNB + 1;     // T row stride (complex): conflict-free row access
 constexpr int YS = CW + 2;      // Y row stride (complex)
 constexpr long long kWait = 1ll << 26;
 
@@ -65,20 +65,6 @@ __device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, do
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a0), "d"(a1), "d"(b0));
 }
-
-__device__ __forceinline__ z64 zrecip(z64 z) {  // Smith's algorithm
-  if (fabs(z.x) >= fabs(z.y)) {
-    if (z.x == 0.0 && z.y == 0.0) return make_double2(0.0, 0.0);
-    const double r = z.y / z.x;
-    const double den = z.x + z.y * r;
-    return make_double2(1.0 / den, -r / den);
-  }
-  const double r = z.x / z.y;
-  const double den = z.x * r + z.y;
-  return make_double2(r / den, -1.0 / den);
-}
-
-__device__ __forceinline__ double cabs1(z64 z) { return fabs(z.x) + fabs(z.y); }
 
 __device__ __forceinline__ uint32_t saddr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -100,21 +86,40 @@ __device__ __forceinline__ int xoff(int npad, int r, int j) {
 struct ClusterSmem {
   // byte offsets inside the dynamic shared memory (base aligned to 1024)
   int npad;
-  size_t x, t, y, piv, colsrc, aff, red_v, red_i, bar, total;
+  size_t x, t, y, piv, colsrc, red_v, red_i, bar, total;
   __host__ __device__ explicit ClusterSmem(int n) {
     npad = (n + 15) & ~15;
-    x = 0;
-    t = x + (size_t)4 * npad * 8 * sizeof(z64);
-    y = t + (size_t)npad * TS * sizeof(z64);
-    piv = y + (size_t)CNB * YS * sizeof(z64);
-    colsrc = piv + (size_t)npad * sizeof(int);
-    aff = colsrc + (size_t)npad * sizeof(int);
-    red_v = aff + (size_t)4 * CNB * sizeof(int);
+    x = 0;                                                  // 4 chunks [npad][8]
+    t = x + (size_t)4 * npad * 8 * sizeof(z64);             // 2 chunks [npad][8]
+    y = t + (size_t)2 * npad * 8 * sizeof(z64);             // [CNB][YS]
+    piv = y + (size_t)CNB * YS * sizeof(z64);               // npad ints
+    colsrc = piv + (size_t)npad * sizeof(int);              // npad ints
+    red_v = colsrc + (size_t)npad * sizeof(int);
     red_i = red_v + (size_t)CWARPS * sizeof(double);
-    bar = (red_i + (size_t)CWARPS * sizeof(int) + 7) & ~(size_t)7;
+    bar = (red_i + (size_t)CWARPS * sizeof(int) + 15) & ~(size_t)15;  // 2 mbarriers
     total = bar + 16 + 1024;  // + alignment slack of the base
   }
 };
+
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kWait; ++it) {
+    uint32_t done = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(saddr(bar)), "r"(parity));
+    if (done) return true;
+  }
+  return false;
+}
 
 template <int C>
 __global__ void __launch_bounds__(CT, 1)
@@ -136,61 +141,44 @@ __global__ void __launch_bounds__(CT, 1)
   z64* Ys = reinterpret_cast<z64*>(base + L.y);
   int* pivrow = reinterpret_cast<int*>(base + L.piv);
   int* colsrc = reinterpret_cast<int*>(base + L.colsrc);
-  int* aff_row = reinterpret_cast<int*>(base + L.aff);
-  int* aff_src = aff_row + 2 * CNB;
   double* red_v = reinterpret_cast<double*>(base + L.red_v);
   int* red_i = reinterpret_cast<int*>(base + L.red_i);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(base + L.bar);
-  __shared__ int s_na, s_sing, s_err;
+  uint64_t* lbar = reinterpret_cast<uint64_t*>(base + L.bar);  // the load of A
+  uint64_t* tbar = lbar + 1;                                    // the panel transforms
+  __shared__ int s_sing, s_first;
   __shared__ z64 prow[CNB], rowk[CNB];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
   const int col0 = rank * CW;  // first global column of this CTA
+  const size_t chunk = (size_t)npad * 8;  // complex elements per 8-column chunk
 
   // ---- load this CTA's 32 columns --------------------------------------
   if (tid == 0) {
-    s_sing = 0x7fffffff;
-    s_err = 0;
-    if (use_tma) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(saddr(bar)));
-      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    }
+    s_sing = 0;
+    s_first = 0x7fffffff;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(saddr(lbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(saddr(tbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
   __syncthreads();
   if (use_tma) {
     if (tid == 0) {
       const uint32_t bytes = 4u * (uint32_t)n * 128u;
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(bar)), "r"(bytes)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(lbar)), "r"(bytes)
                    : "memory");
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int x = 2 * (col0 + 8 * i);  // in doubles: 16-byte aligned
         asm volatile(
             "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-            " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(saddr(Xs + (size_t)i * npad * 8)),
-            "l"(&tmap), "r"(x), "r"(0), "r"((int)b), "r"(saddr(bar))
+            " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(saddr(Xs + i * chunk)),
+            "l"(&tmap), "r"(x), "r"(0), "r"((int)b), "r"(saddr(lbar))
             : "memory");
       }
     }
-    if (warp == 0) {
-      bool ok = false;
-      for (long long it = 0; it < kWait && !ok; ++it) {
-        uint32_t done = 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(saddr(bar)));
-        ok = done != 0;
-      }
-      if (!ok && lane == 0) {
-        s_err = 1;
-        atomicExch(&g_zinv_cluster_error, 1);
-      }
-    }
+    if (warp == 0 && !mbar_wait_bounded(lbar, 0) && lane == 0) atomicExch(&g_zinv_cluster_error, 1);
   } else {
     const z64* a = at<const z64>(A, b);
     for (int idx = tid; idx < n * CW; idx += CT) {
@@ -202,199 +190,120 @@ __global__ void __launch_bounds__(CT, 1)
   cluster.sync();  // every CTA resident and loaded before any DSMEM access
 
   // ---- panels -----------------------------------------------------------
+  uint32_t tphase = 0;
   for (int k0 = 0; k0 < n; k0 += CNB) {
     const int owner = k0 / CW, kl = k0 - owner * CW;
     const int nbp = min(CNB, n - k0);
     const bool own = rank == owner;
+    const uint32_t tbytes = (uint32_t)(2 * chunk * sizeof(z64)) + CNB * sizeof(int);
 
     if (own) {
-      // Factor columns [kl, kl + nbp) of X in place (rows 0..n-1). Row k
-      // receives the scaled pivot row, row p the eliminated old row k.
-      double best = -1.0;
-      int besti = k0;
-      for (int r = k0 + tid; r < n; r += CT) {
-        const double v = cabs1(Xs[xoff(npad, r, kl)]);
-        if (v > best || (v == best && r < besti)) {
-          best = v;
-          besti = r;
-        }
-      }
-      for (int kk = 0; kk < nbp; ++kk) {
-        const int k = k0 + kk;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const double ov = __shfl_xor_sync(0xffffffffu, best, off);
-          const int oi = __shfl_xor_sync(0xffffffffu, besti, off);
-          if (ov > best || (ov == best && oi < besti)) {
-            best = ov;
-            besti = oi;
-          }
-        }
-        // (the reads below come before the next barrier, the next writes after it)
-        if (lane == 0) {
-          red_v[warp] = best;
-          red_i[warp] = besti;
-        }
-        __syncthreads();
-        best = red_v[0];
-        besti = red_i[0];
-#pragma unroll
-        for (int w = 1; w < CWARPS; ++w) {
-          const double ov = red_v[w];
-          const int oi = red_i[w];
-          if (ov > best || (ov == best && oi < besti)) {
-            best = ov;
-            besti = oi;
-          }
-        }
-        const int p = besti;
-        if (best <= 0.0 && tid == 0 && s_sing == 0x7fffffff) s_sing = k + 1;
-        const z64 dpiv = zrecip(Xs[xoff(npad, p, kl + kk)]);
-        if (tid < CNB) {
-          rowk[tid] = Xs[xoff(npad, k, kl + tid)];
-          prow[tid] = (tid == kk) ? dpiv : zmul(Xs[xoff(npad, p, kl + tid)], dpiv);
-        }
-        if (tid == 0) pivrow[k] = p;
-        __syncthreads();
-        best = -1.0;
-        besti = k + 1;
-        for (int r = tid; r < n; r += CT) {
-          if (r == k) {
-#pragma unroll
-            for (int c = 0; c < CNB; ++c) Xs[xoff(npad, r, kl + c)] = prow[c];
-            continue;
-          }
-          const bool swapped = r == p;  // row p receives the old row k
-          const z64 f = swapped ? rowk[kk] : Xs[xoff(npad, r, kl + kk)];
-#pragma unroll
-          for (int c = 0; c < CNB; ++c) {
-            if (c == kk) continue;
-            const z64 v = swapped ? rowk[c] : Xs[xoff(npad, r, kl + c)];
-            const z64 q = prow[c];
-            Xs[xoff(npad, r, kl + c)] = make_double2(v.x - (f.x * q.x - f.y * q.y), v.y - (f.x * q.y + f.y * q.x));
-          }
-          const z64 m = zmul(f, dpiv);
-          Xs[xoff(npad, r, kl + kk)] = make_double2(-m.x, -m.y);
-          if (kk + 1 < nbp && r > k) {
-            const double v = cabs1(Xs[xoff(npad, r, kl + kk + 1)]);
-            if (v > best || (v == best && r < besti)) {
-              best = v;
-              besti = r;
-            }
-          }
-        }
-      }
+      gj_factor_panel16(
+          n, k0, nbp, [&](int r, int c) { return Xs[xoff(npad, r, kl + c)]; },
+          [&](int r, int c, z64 v) { Xs[xoff(npad, r, kl + c)] = v; }, pivrow, prow, rowk, red_v, red_i,
+          &s_sing);
+      // the panel's stores must be visible to the bulk copies below
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    } else if (tid == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(tbar)), "r"(tbytes)
+                   : "memory");
     }
-    // The panel transform and its pivots are ready in the owner's memory.
+    // Every CTA has finished reading the previous transform and the owner
+    // has factored this panel.
     cluster_arrive();
     cluster_wait();
-
-    // Pull T = X_owner[:, kl:kl+nbp] (rows >= n and columns >= nbp as zero)
-    // and the panel's pivots.
-    {
-      const z64* rX = cluster.map_shared_rank(Xs, owner);
-      const int* rP = cluster.map_shared_rank(pivrow, owner);
-      const int total = npad * CNB;  // <= 256 x 16 = 8 per thread
-      z64 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int idx = tid + u * CT, r = idx / CNB, c = idx % CNB;
-        v[u] = (idx < total && r < n && c < nbp) ? rX[xoff(npad, r, kl + c)] : make_double2(0.0, 0.0);
+    if (own && tid == 0) {
+      // The transform (columns kl..kl+15: two whole chunks) and its pivots
+      // to every other CTA of the cluster (bulk copies, no multicast).
+      const uint32_t src_t = saddr(Xs + (size_t)(kl >> 3) * chunk);
+      const uint32_t src_p = saddr(pivrow + k0);
+      for (int r = 0; r < C; ++r) {
+        if (r == rank) continue;
+        const uint32_t mb = cluster_addr(saddr(tbar), r);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                cluster_addr(saddr(Ts), r)),
+            "r"(src_t), "r"((uint32_t)(2 * chunk * sizeof(z64))), "r"(mb)
+            : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                cluster_addr(saddr(pivrow + k0), r)),
+            "r"(src_p), "r"((uint32_t)(CNB * sizeof(int))), "r"(mb)
+            : "memory");
       }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int idx = tid + u * CT;
-        if (idx < total) Ts[(idx / CNB) * TS + idx % CNB] = v[u];
-      }
-      if (tid < nbp && !own) pivrow[k0 + tid] = rP[k0 + tid];
     }
-    __syncthreads();
-
-    // Row interchanges of the panel as one permutation of the affected rows
-    // (row aff_row[a] receives the old content of row aff_src[a]).
-    if (tid == 0) {
-      int na = 0;
-      for (int kk = 0; kk < nbp; ++kk) {
-        const int k = k0 + kk, p = pivrow[k];
-        int ik = -1, ip = -1;
-        for (int u = 0; u < na; ++u) {
-          if (aff_row[u] == k) ik = u;
-          if (aff_row[u] == p) ip = u;
-        }
-        if (ik < 0) {
-          ik = na++;
-          aff_row[ik] = k;
-          aff_src[ik] = k;
-        }
-        if (ip < 0) {
-          ip = na++;
-          aff_row[ip] = p;
-          aff_src[ip] = p;
-        }
-        const int t = aff_src[ik];
-        aff_src[ik] = aff_src[ip];
-        aff_src[ip] = t;
-      }
-      s_na = na;
-    }
-    __syncthreads();
-    {
-      const int na = s_na;
-      z64 v[2];
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int li = tid + u * CT, a = li / CW, j = li % CW;
-        const bool panel = own && j >= kl && j < kl + CNB;
-        if (a < na && !panel) v[u] = Xs[xoff(npad, aff_src[a], j)];
-      }
+    if (!own) {
+      if (warp == 0 && !mbar_wait_bounded(tbar, tphase) && lane == 0) atomicExch(&g_zinv_cluster_error, 1);
+      tphase ^= 1u;
       __syncthreads();
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int li = tid + u * CT, a = li / CW, j = li % CW;
-        const bool panel = own && j >= kl && j < kl + CNB;
-        if (a < na && !panel) Xs[xoff(npad, aff_row[a], j)] = v[u];
-      }
     }
-    __syncthreads();
-    // Pivot rows of this CTA's (non-panel) columns.
-    for (int idx = tid; idx < CNB * CW; idx += CT) {
-      const int kk = idx / CW, j = idx % CW;
+    const z64* T = own ? Xs + (size_t)(kl >> 3) * chunk : Ts;
+
+    // Row interchanges of this CTA's other columns (lane = column), then the
+    // pivot rows Y.
+    if (warp == 0) {
+      const int j = lane;
       const bool panel = own && j >= kl && j < kl + CNB;
-      Ys[kk * YS + j] = (kk < nbp && !panel) ? Xs[xoff(npad, k0 + kk, j)] : make_double2(0.0, 0.0);
+      if (!panel) {
+        for (int kk = 0; kk < nbp; ++kk) {
+          const int k = k0 + kk, p = pivrow[k];
+          if (p != k) {
+            const z64 a = Xs[xoff(npad, k, j)], c = Xs[xoff(npad, p, j)];
+            Xs[xoff(npad, k, j)] = c;
+            Xs[xoff(npad, p, j)] = a;
+          }
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < CNB; ++kk)
+        Ys[kk * YS + j] = (kk < nbp && !panel) ? Xs[xoff(npad, k0 + kk, j)] : make_double2(0.0, 0.0);
     }
     __syncthreads();
 
-    // Update: 16-row slices x 8-column tiles, 4 complex MMAs per k step.
+    // Update: warp w takes rows [16 w, 16 w + 16) of a pair of 8-column
+    // tiles at a time (four independent accumulator chains); the owner skips
+    // the pair that holds the panel (kl is 0 or 16: exactly one pair).
     const int mtiles = (n + 15) >> 4;
-    for (int item = warp; item < mtiles * (CW / 8); item += CWARPS) {
-      const int mt = item / (CW / 8), jt = item % (CW / 8);
-      const int r0 = mt * 16, j0 = jt * 8;
-      if (own && j0 >= kl && j0 < kl + CNB) continue;  // the panel holds T
-      double cre[4], cim[4];
+    for (int mt = warp; mt < mtiles; mt += CWARPS) {
+      const int r0 = mt * 16;
+      const int ra = r0 + g;
+#pragma unroll 1
+      for (int jp = 0; jp < 2; ++jp) {
+        if (own && jp * 16 == kl) continue;
+        double cre[2][4], cim[2][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = r0 + g + ((q >> 1) << 3);
-        const int j = j0 + 2 * tq + (q & 1);
-        z64 v = make_double2(0.0, 0.0);
-        if (r < n && !(r >= k0 && r < k0 + nbp)) v = Xs[xoff(npad, r, j)];
-        cre[q] = v.x;
-        cim[q] = v.y;
-      }
+        for (int t = 0; t < 2; ++t)
 #pragma unroll
-      for (int k4 = 0; k4 < CNB; k4 += 4) {
-        const z64 v0 = Ts[(r0 + g) * TS + k4 + tq];
-        const z64 v1 = Ts[(r0 + g + 8) * TS + k4 + tq];
-        const z64 bv = Ys[(k4 + tq) * YS + j0 + g];
-        mma_f64(cre, v0.x, v1.x, bv.x);
-        mma_f64(cim, v0.x, v1.x, bv.y);
-        mma_f64(cre, -v0.y, -v1.y, bv.y);
-        mma_f64(cim, v0.y, v1.y, bv.x);
-      }
+          for (int q = 0; q < 4; ++q) {
+            const int r = ra + ((q >> 1) << 3);
+            const int j = jp * 16 + t * 8 + 2 * tq + (q & 1);
+            z64 v = make_double2(0.0, 0.0);
+            if (r < n && !(r >= k0 && r < k0 + nbp)) v = Xs[xoff(npad, r, j)];
+            cre[t][q] = v.x;
+            cim[t][q] = v.y;
+          }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = r0 + g + ((q >> 1) << 3);
-        const int j = j0 + 2 * tq + (q & 1);
-        if (r < n) Xs[xoff(npad, r, j)] = make_double2(cre[q], cim[q]);
+        for (int k4 = 0; k4 < CNB; k4 += 4) {
+          const int ka = k4 + tq;
+          const z64 v0 = T[(ka >> 3) * chunk + ra * 8 + ((ka & 7) ^ (ra & 7))];
+          const z64 v1 = T[(ka >> 3) * chunk + (ra + 8) * 8 + ((ka & 7) ^ ((ra + 8) & 7))];
+#pragma unroll
+          for (int t = 0; t < 2; ++t) {
+            const z64 bv = Ys[ka * YS + jp * 16 + t * 8 + g];
+            mma_f64(cre[t], v0.x, v1.x, bv.x);
+            mma_f64(cim[t], v0.x, v1.x, bv.y);
+            mma_f64(cre[t], -v0.y, -v1.y, bv.y);
+            mma_f64(cim[t], v0.y, v1.y, bv.x);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = ra + ((q >> 1) << 3);
+            const int j = jp * 16 + t * 8 + 2 * tq + (q & 1);
+            if (r < n) Xs[xoff(npad, r, j)] = make_double2(cre[t][q], cim[t][q]);
+          }
       }
     }
     __syncthreads();
@@ -413,7 +322,7 @@ __global__ void __launch_bounds__(CT, 1)
         colsrc[p] = t;
       }
     }
-    if (s_sing != 0x7fffffff) atomicMin(cluster.map_shared_rank(&s_sing, 0), s_sing);
+    if (s_sing != 0) atomicMin(cluster.map_shared_rank(&s_first, 0), s_sing);
   }
   __syncthreads();
   cluster.sync();  // every update and every first-singular report done
@@ -439,7 +348,7 @@ __global__ void __launch_bounds__(CT, 1)
       }
     }
   }
-  if (rank == 0 && tid == 0 && info != nullptr && s_sing != 0x7fffffff && info[b] == 0) info[b] = s_sing;
+  if (rank == 0 && tid == 0 && info != nullptr && s_first != 0x7fffffff && info[b] == 0) info[b] = s_first;
   cluster.sync();  // no CTA leaves while another still reads its shared memory
 }
 

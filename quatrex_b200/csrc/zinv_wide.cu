@@ -305,11 +305,12 @@ bool zinv_prefers_cluster(int n, int64_t batch) {
   if (g_inverse_path == 3) return true;
   if (g_inverse_path != 0) return false;
   // A cluster per matrix (ceil(n / 32) CTAs, one per SM at n = 256) finishes
-  // one matrix far sooner than one CTA streaming it through HBM, but holds
-  // several SMs for it: it wins while the batch keeps few clusters waiting.
+  // one matrix 2.2x sooner than one CTA streaming it through HBM (0.59 vs
+  // 1.31 ms at n = 256), but holds C SMs for it, and the GPU co-schedules
+  // only about half of the SM count in clusters of 8: measured on B200, it
+  // wins while batch x C stays within half the SMs (n = 256: batch <= 9).
   const int c = (n + 31) / 32;
-  const int resident = num_sms() / c;
-  return batch <= 4 * (int64_t)resident;
+  return batch * c * 2 <= (int64_t)num_sms();
 }
 
 bool zinv_prefers_wide(int n, int64_t batch) {
