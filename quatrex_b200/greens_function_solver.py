@@ -215,14 +215,23 @@ class RGF(GFSolver):
     def _selected_solve_pipelined(self, a, sigma_lesser, sigma_greater, obc_blocks, xl, xg, xr, current, sizes,
                                   slices, out, return_retarded, return_current):
         """selected_solve for host (CPU torch) containers with more than one
-        batch: batch k+1 is uploaded on a copy stream and batch k-1 written
-        back on a third stream while batch k is solved. Same results and
-        conventions; a singular block raises after the last batch."""
+        batch: uploads run on a copy stream two batches ahead and write-backs
+        on a third stream while a batch is solved. The first and the last
+        batch are split in halves so that the upload before the first solve
+        and the write-back after the last one (the parts nothing overlaps)
+        are short. The copy streams persist across calls, so the caching
+        allocator reuses their buffers instead of allocating new ones each
+        call. Same results and conventions; a singular block raises after the
+        last batch."""
         lib = _native.load()
         device = self._dev()
         n = int(sigma_lesser.num_blocks)
         comp = torch.cuda.current_stream(device)
-        up_s, down_s = torch.cuda.Stream(device), torch.cuda.Stream(device)
+        up_s, down_s = _copy_streams(device)
+        up_s.wait_stream(comp)
+        down_s.wait_stream(comp)
+        slices = _split_ends(slices)
+        sizes = np.diff(slices)
         sym_l = bool(getattr(xl, "symmetry", False))
         sym_g = bool(getattr(xg, "symmetry", False))
         flags = _native.QTX_SOLVE_SYMMETRIC_OUT if (sym_l or sym_g) else 0
@@ -245,17 +254,17 @@ class RGF(GFSolver):
                 ev.record(up_s)
             return sl, views, obcs, obc_keep, ev
 
-        nxt = stage(0)
+        staged = [stage(b) for b in range(min(2, len(sizes)))]
         for b in range(len(sizes)):
-            sl, views, obcs, obc_keep, ev = nxt
+            sl, views, obcs, obc_keep, ev = staged.pop(0)
+            if b + 2 < len(sizes):
+                staged.append(stage(b + 2))
             comp.wait_event(ev)
-            if b + 1 < len(sizes):
-                nxt = stage(b + 1)
             A, SL, SG, XL, XG, XR = views
             batch = A.batch
             cur = torch.zeros((batch, n + 1), dtype=torch.complex128, device=device) if return_current else None
-            abi = [v.abi() if v is not None else None for v in views]
             info = torch.zeros(batch, dtype=torch.int32, device=device)
+            abi = [v.abi() if v is not None else None for v in views]
             _solve_call(lib, self.precision, abi, obcs, cur, info,
                         lambda nb: workspace_pool.get(nb, device, "rgf"), flags, batch,
                         ctypes.c_void_p(comp.cuda_stream), device)
@@ -387,6 +396,29 @@ def _solve_call(lib, precision, abi, obcs, cur, info, ws_getter, flags, batch, s
                 if q.ptr and arr[i].ptr:
                     r, c = shapes[kk][i]
                     _convert(lib, r, c, batch, q, c64, arr[i], c128, stream)
+
+
+_streams: dict = {}
+
+
+def _copy_streams(device: torch.device):
+    """The upload and write-back streams of a device (created once)."""
+    key = (device.type, device.index)
+    if key not in _streams:
+        _streams[key] = (torch.cuda.Stream(device), torch.cuda.Stream(device))
+    return _streams[key]
+
+
+def _split_ends(slices) -> np.ndarray:
+    """Batch boundaries with the first and the last batch halved."""
+    b = [int(x) for x in slices]
+    if len(b) >= 3:  # at least two batches
+        first, last = b[1] - b[0], b[-1] - b[-2]
+        if last >= 2:
+            b.insert(len(b) - 1, b[-2] + last // 2)
+        if first >= 2:
+            b.insert(1, b[0] + first // 2)
+    return np.asarray(b)
 
 
 def _on_host(m) -> bool:
