@@ -11,7 +11,11 @@
 // global loads and stores stay coalesced. Reductions use warp shuffles and
 // one shared-memory combine per CTA; one CTA reduces one stack entry, so
 // results are deterministic.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace qtx {
 namespace {
@@ -133,19 +137,26 @@ __device__ __forceinline__ V block_sum(V v, V* red) {
   return s;
 }
 
-// One CTA per stack entry: Tr(X Y) = sum_{r,c} X[r][c] Y[c][r], via 32x32
-// tiles (Y tile staged transposed).
+// Tr(X Y) = sum_{r,c} X[r][c] Y[c][r], via 32x32 tiles (Y tile staged
+// transposed). A stack entry is reduced by the S CTAs of one thread-block
+// cluster (S = 1 for large batches): CTA s takes the row tiles s, s + S, ...
+// and the S partial sums are added in rank order by rank 0 through
+// distributed shared memory, so the result does not depend on timing.
 template <typename T>
 __global__ void __launch_bounds__(256) trace_kernel(int n, int64_t batch, MatRef X, MatRef Y, z64 coef,
                                                     z64* res, int64_t rs, int64_t roff, int accumulate) {
   __shared__ z64 tile[TILE][TILE + 1];
   __shared__ double red[8];
+  __shared__ double part[2];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int S = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+  const int64_t b = blockIdx.x / S;  // uniform within a cluster
+  if (b < batch) {
     const T* x = at<const T>(X, b);
     const T* y = at<const T>(Y, b);
     double sre = 0.0, sim = 0.0;
-    for (int r0 = 0; r0 < n; r0 += TILE)
+    for (int r0 = rank * TILE; r0 < n; r0 += S * TILE)
       for (int c0 = 0; c0 < n; c0 += TILE) {
         __syncthreads();
 #pragma unroll
@@ -169,11 +180,23 @@ __global__ void __launch_bounds__(256) trace_kernel(int n, int64_t batch, MatRef
     sre = block_sum(sre, red);
     sim = block_sum(sim, red);
     if (threadIdx.x == 0) {
-      const z64 v = zmul(coef, make_double2(sre, sim));
-      z64* o = res + b * rs + roff;
-      *o = accumulate ? zadd(*o, v) : v;
+      part[0] = sre;
+      part[1] = sim;
     }
   }
+  cluster.sync();
+  if (b < batch && rank == 0 && threadIdx.x == 0) {
+    double tre = 0.0, tim = 0.0;
+    for (int q = 0; q < S; ++q) {
+      const double* pq = cluster.map_shared_rank(part, q);
+      tre += pq[0];
+      tim += pq[1];
+    }
+    const z64 v = zmul(coef, make_double2(tre, tim));
+    z64* o = res + b * rs + roff;
+    *o = accumulate ? zadd(*o, v) : v;
+  }
+  cluster.sync();  // the partials stay readable until rank 0 has summed them
 }
 
 // delta[b] = sqrt(sum (|x| + |y|)^2) / 2.
@@ -298,8 +321,24 @@ int trace_t(int n, int64_t batch, MatRef X, MatRef Y, z64 coef, z64* result, int
             int64_t roff, int accumulate, cudaStream_t s) {
   if (n <= 0 || batch <= 0) return QTX_OK;
   ProfScope prof(QTX_KERNEL_REDUCE, 2.0 * sizeof(T) * n * n * (double)batch, s);
-  trace_kernel<T><<<grid_x(batch), 256, 0, s>>>(n, batch, X, Y, coef, result, rstride, roff, accumulate);
-  QTX_CHECK_LAUNCH();
+  // CTAs per stack entry: enough for two waves of the SMs, at most 8 (a
+  // portable cluster) and at most one per 32-row tile.
+  int S = 1;
+  while (S < 8 && (int64_t)S * 2 * batch <= 2 * 148 && S * TILE < n) S *= 2;
+  if ((int64_t)batch * S > 0x7fffffffll) S = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(batch * S), 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  QTX_CHECK_CUDA(cudaLaunchKernelEx(&cfg, trace_kernel<T>, n, batch, X, Y, coef, result, rstride, roff, accumulate));
   return QTX_OK;
 }
 
