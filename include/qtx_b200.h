@@ -272,6 +272,23 @@ int qtx_sancho_rubio_multi_async(int n, int num_systems, const int64_t* batches,
                                  int* d_iterations, int* d_converged, int* info, void* workspace,
                                  size_t workspace_bytes, qtx_stream stream);
 
+/* Workspace bytes for qtx_beyn_moments. */
+size_t qtx_beyn_moments_workspace(int n, int64_t batch, int num_quad_points);
+
+/* Moments of Beyn's contour integral for the spectral open-boundary
+ * condition, qttools nevp/beyn.py:166-220 (Beyn._contour_integrate, with
+ * kernels/operator.py:117-181): for T(z) = a_ji / z + a_ii + a_ij z and the
+ * quadrature points z_j = r exp(2 pi i (j + 1.5) / nq), j < nq, on the
+ * circles r = r_o and r = r_i, weight w = 1 / nq,
+ *   q0 = sum_j w (z_o,j T(z_o,j)^-1 - z_i,j T(z_i,j)^-1),
+ *   q1 = sum_j w (z_o,j^2 T(z_o,j)^-1 - z_i,j^2 T(z_i,j)^-1),
+ * for every stack entry (2 nq batched n x n inverses per entry). info
+ * (device int[batch], optional): 1-based index of the first singular
+ * operator of the entry (outer circle first), 0 if none. */
+int qtx_beyn_moments(int n, int64_t batch, qtx_mat a_ji, qtx_mat a_ii, qtx_mat a_ij, double r_o,
+                     double r_i, int num_quad_points, qtx_mat q0, qtx_mat q1, int* info,
+                     void* workspace, size_t workspace_bytes, qtx_stream stream);
+
 /* Workspace bytes sufficient for qtx_contact_self_energy, qtx_obc_refine
  * and qtx_transmission (square n x n blocks) on `batch` entries. */
 size_t qtx_obc_workspace(int n, int64_t batch);

@@ -3,8 +3,9 @@ NEGF hot path behind the qttools solver interfaces.
 
 * :class:`RGF` -- drop-in for ``qttools.greens_function_solver.RGF``
   (``selected_inv`` / ``selected_solve``);
-* :class:`SanchoRubio`, :class:`OBCSystem` -- drop-ins for the qttools OBC
-  solver and its memoizing wrapper;
+* :class:`SanchoRubio`, :class:`Spectral` (with the :class:`Beyn` NEVP
+  solver), :class:`OBCSystem` -- drop-ins for the qttools OBC solvers and
+  their memoizing wrapper;
 * :class:`DSDBCOO` -- torch-backed block-sorted COO stack with the qttools
   block / stack indexers;
 * :class:`EnergyPointSolver` -- the whole per-energy unit (OBC + selected
@@ -20,11 +21,12 @@ from .negf import EnergyPointSolver, flops_per_energy
 from .obc import (OBCSolver, OBCSystem, SanchoRubio, contact_self_energy, fixed_point_refine, inverse,
                   transmission)
 from .observables import density
+from .spectral import Beyn, Spectral
 
 __all__ = [
     "DSDBCOO", "RGF", "GFSolver", "OBCBlocks", "EnergyPointSolver", "flops_per_energy", "OBCSolver",
     "OBCSystem", "SanchoRubio", "contact_self_energy", "fixed_point_refine", "inverse", "transmission",
-    "density",
+    "density", "Beyn", "Spectral",
 ]
 
 __version__ = "0.1.0"

@@ -183,3 +183,37 @@ def random_bt_dense(block_sizes, seed: int = 0, density: float = 0.5) -> np.ndar
     for i in range(size):
         arr[i, i] = (1 + 1j) + arr[i, :].sum()
     return arr
+
+
+def strip_lead(width: int, slices: int, energies, seed: int = 0, eta: float = ETA, disorder: float = 0.3):
+    """Boundary blocks of a semi-infinite strip lead: a square lattice
+    ``width`` sites wide with nearest-neighbour hopping -1, onsite energies
+    uniform in [-disorder/2, disorder/2] (``default_rng(seed)``), cut into
+    blocks of ``slices`` consecutive slices (block size width x slices).
+    Returns ``(a_ii, a_ij, a_ji)`` of ``A = (E + i eta) I - H`` as
+    (E, b, b) complex128 stacks. The coupling between blocks has rank
+    ``width``, so at most 2 x width of the 2 b eigenmodes of the lead are
+    finite and nonzero, and only the propagating and slowly decaying ones lie
+    in an annulus around the unit circle: the regime that contour-integral
+    (Beyn) OBC solvers with a subspace of a few modes are built for."""
+    rng = np.random.default_rng(seed)
+    b = width * slices
+    h = np.diag(rng.uniform(-disorder / 2, disorder / 2, b)).astype(np.complex128)
+    for s_ in range(slices):
+        for c in range(width - 1):
+            i = s_ * width + c
+            h[i, i + 1] = h[i + 1, i] = -1.0
+        if s_ + 1 < slices:
+            for c in range(width):
+                i = s_ * width + c
+                h[i, i + width] = h[i + width, i] = -1.0
+    t = np.zeros((b, b), dtype=np.complex128)  # H_{i,i+1}: last slice -> next block's first slice
+    for c in range(width):
+        t[(slices - 1) * width + c, c] = -1.0
+    e = np.asarray(energies, dtype=np.float64)
+    z = (e + 1j * eta)[:, None, None]
+    eye = np.eye(b, dtype=np.complex128)
+    a_ii = z * eye - h
+    a_ij = np.broadcast_to(-t, (e.size, b, b)).copy()
+    a_ji = np.broadcast_to(-t.conj().T, (e.size, b, b)).copy()
+    return a_ii, a_ij, a_ji
