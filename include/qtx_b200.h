@@ -357,6 +357,21 @@ int qtx_assemble_energies(int64_t batch, const double* energies, double eta, voi
 int qtx_assemble_diag(int n, int64_t batch, qtx_mat h, const void* z, qtx_mat out,
                       qtx_stream stream);
 
+/* System matrix of the electron solve in one pass, quatrex
+ * electron/solver.py:668-709 (ElectronSolver._assemble_system_matrix with
+ * _subtract_hamiltonian_and_self_energy, :611-665; no overlap matrix):
+ *   A_ij = delta_ij (z_b I - diag(V_i)) - H_ij - Sigma^R_ij
+ *          - (Sigma^>_ij - Sigma^<_ij) / 2
+ * for every block of the block-tridiagonal a (a NULL output block is not
+ * written). h: Hamiltonian blocks (stride 0 for energy-independent ones);
+ * potential: device double[sum(block_sizes)] or NULL; z: device
+ * complex128[batch] energies E + i eta; sigma_*: scattering self-energies
+ * (Sigma^R is its Hermitian part), NULL or NULL blocks for zero. */
+int qtx_assemble_system(const qtx_bt* h, const double* potential, const void* z,
+                        const qtx_bt* sigma_retarded, const qtx_bt* sigma_lesser,
+                        const qtx_bt* sigma_greater, const qtx_bt* a, int64_t batch,
+                        qtx_stream stream);
+
 /* Launch profiler. Kernel classes: */
 enum qtx_kernel_class {
   QTX_KERNEL_ZGEMM = 0,    /* batched complex GEMM; work = 8 m n k flops */

@@ -17,14 +17,14 @@ All arithmetic runs in ``lib/libqtx_b200.so`` (hand-written CUDA, C ABI in
 
 from .datastructures import DSDBCOO
 from .greens_function_solver import RGF, GFSolver, OBCBlocks
-from .negf import EnergyPointSolver, flops_per_energy
+from .negf import EnergyPointSolver, ScatteringSelfEnergy, flops_per_energy
 from .obc import (OBCSolver, OBCSystem, SanchoRubio, contact_self_energy, fixed_point_refine, inverse,
                   transmission)
 from .observables import density
 from .spectral import Beyn, Spectral
 
 __all__ = [
-    "DSDBCOO", "RGF", "GFSolver", "OBCBlocks", "EnergyPointSolver", "flops_per_energy", "OBCSolver",
+    "DSDBCOO", "RGF", "GFSolver", "OBCBlocks", "EnergyPointSolver", "ScatteringSelfEnergy", "flops_per_energy", "OBCSolver",
     "OBCSystem", "SanchoRubio", "contact_self_energy", "fixed_point_refine", "inverse", "transmission",
     "density", "Beyn", "Spectral",
 ]

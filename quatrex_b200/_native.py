@@ -112,6 +112,8 @@ SIGNATURES = {
     "qtx_profile_read": (c_int, [c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]),
     "qtx_assemble_energies": (c_int, [c_int64, c_void_p, c_double, c_void_p, c_void_p]),
     "qtx_assemble_diag": (c_int, [c_int, c_int64, QtxMat, c_void_p, QtxMat, c_void_p]),
+    "qtx_assemble_system": (c_int, [POINTER(QtxBT), c_void_p, c_void_p, POINTER(QtxBT), POINTER(QtxBT),
+                                    POINTER(QtxBT), POINTER(QtxBT), c_int64, c_void_p]),
 }
 
 _lib = None

@@ -190,3 +190,110 @@ extern "C" int qtx_copy_ranges(void* dst, int64_t dst_row_bytes, const void* src
   }
   return QTX_OK;
 }
+
+// System-matrix assembly in one pass (quatrex electron/solver.py:668-709
+// with _subtract_hamiltonian_and_self_energy, :611-665, no overlap):
+//   A_ij = delta_ij (z_b I - diag(V_i)) - H_ij - Sigma^R_ij
+//          - 1/2 (Sigma^>_ij - Sigma^<_ij)
+// for every tridiagonal block (i, j) of a batch. The reference builds the
+// same matrix in five passes over the DSDBCOO data (zero, unit diagonal,
+// energy scale, potential, self-energy and Hamiltonian subtraction); here
+// each output block is written once from one read of each input.
+namespace qtx {
+namespace {
+struct AsmArgs {
+  MatRef out, h, sr, sl, sg;
+  const double* v;  // potential of the block's rows (diagonal blocks), or null
+  const z64* z;     // complex energies (diagonal blocks), or null
+  int m, n;
+  int64_t batch;
+};
+
+__global__ void assemble_block_kernel(const AsmArgs a) {
+  const int64_t per = (int64_t)a.m * a.n;
+  const int64_t total = per * a.batch;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / per, e = i % per;
+    const int r = (int)(e / a.n), c = (int)(e % a.n);
+    z64 o = make_double2(0.0, 0.0);
+    if (a.z != nullptr && r == c) {
+      o = a.z[b];
+      if (a.v != nullptr) o.x -= a.v[r];
+    }
+    if (!a.h.null()) o = zsub(o, at<const z64>(a.h, b)[(int64_t)r * a.h.ld + c]);
+    if (!a.sr.null()) o = zsub(o, at<const z64>(a.sr, b)[(int64_t)r * a.sr.ld + c]);
+    if (!a.sg.null()) {
+      const z64 g = at<const z64>(a.sg, b)[(int64_t)r * a.sg.ld + c];
+      o = make_double2(o.x - 0.5 * g.x, o.y - 0.5 * g.y);
+    }
+    if (!a.sl.null()) {
+      const z64 l = at<const z64>(a.sl, b)[(int64_t)r * a.sl.ld + c];
+      o = make_double2(o.x + 0.5 * l.x, o.y + 0.5 * l.y);
+    }
+    at<z64>(a.out, b)[(int64_t)r * a.out.ld + c] = o;
+  }
+}
+}  // namespace
+}  // namespace qtx
+
+extern "C" int qtx_assemble_system(const qtx_bt* h, const double* potential, const void* z,
+                                   const qtx_bt* sigma_retarded, const qtx_bt* sigma_lesser,
+                                   const qtx_bt* sigma_greater, const qtx_bt* a, int64_t batch,
+                                   qtx_stream stream) {
+  try {
+    if (batch <= 0) return QTX_OK;
+    if (h == nullptr || a == nullptr || z == nullptr || h->num_blocks <= 0 || a->num_blocks != h->num_blocks ||
+        h->block_sizes == nullptr || a->block_sizes == nullptr) {
+      set_error("qtx_assemble_system: invalid arguments");
+      return QTX_ERR_ARG;
+    }
+    const int N = h->num_blocks;
+    for (const qtx_bt* t : {sigma_retarded, sigma_lesser, sigma_greater}) {
+      if (t != nullptr && (t->num_blocks != N || t->block_sizes == nullptr)) {
+        set_error("qtx_assemble_system: self-energy layout differs from the Hamiltonian");
+        return QTX_ERR_ARG;
+      }
+    }
+    std::vector<int64_t> off(N + 1, 0);
+    for (int i = 0; i < N; ++i) {
+      if (h->block_sizes[i] <= 0 || a->block_sizes[i] != h->block_sizes[i]) {
+        set_error("qtx_assemble_system: block sizes differ");
+        return QTX_ERR_ARG;
+      }
+      off[i + 1] = off[i] + h->block_sizes[i];
+    }
+    auto pick = [](const qtx_bt* t, int which, int k) -> MatRef {
+      if (t == nullptr) return MatRef{};
+      const qtx_mat* arr = which == 0 ? t->diag : (which == 1 ? t->upper : t->lower);
+      return arr == nullptr ? MatRef{} : from_abi(arr[k]);
+    };
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int i = 0; i < N; ++i) {
+      for (int which = 0; which < 3; ++which) {
+        if (which > 0 && i + 1 >= N) continue;
+        AsmArgs g;
+        g.out = pick(a, which, i);
+        if (g.out.null()) continue;  // block not wanted
+        g.h = pick(h, which, i);
+        g.sr = pick(sigma_retarded, which, i);
+        g.sl = pick(sigma_lesser, which, i);
+        g.sg = pick(sigma_greater, which, i);
+        g.m = which == 2 ? h->block_sizes[i + 1] : h->block_sizes[i];
+        g.n = which == 1 ? h->block_sizes[i + 1] : h->block_sizes[i];
+        g.z = which == 0 ? static_cast<const z64*>(z) : nullptr;
+        g.v = which == 0 && potential != nullptr ? potential + off[i] : nullptr;
+        g.batch = batch;
+        const int64_t total = (int64_t)g.m * g.n * batch;
+        const int ins = 1 + !g.h.null() + !g.sr.null() + !g.sl.null() + !g.sg.null();
+        ProfScope prof(QTX_KERNEL_FORMAT, 16.0 * ins * (double)total, s);
+        assemble_block_kernel<<<blocks_for(total), 256, 0, s>>>(g);
+        QTX_CHECK_LAUNCH();
+      }
+    }
+    return QTX_OK;
+  } catch (const std::exception& e) {
+    set_error(std::string("qtx_assemble_system: internal error: ") + e.what());
+    return QTX_ERR_ARG;
+  }
+}

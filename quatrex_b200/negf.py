@@ -47,6 +47,19 @@ def _bcast(t: torch.Tensor) -> QtxMat:
 
 
 @dataclass
+class ScatteringSelfEnergy:
+    """Scattering self-energies of one batch, as the electron solve of an
+    SCBA iteration receives them (quatrex electron/solver.py:756-888):
+    ``retarded`` (its Hermitian part), ``lesser`` and ``greater`` are each
+    ``(diag, upper, lower)`` device complex128 stacks of shapes (N, B, b, b),
+    (N-1, B, b, b), (N-1, B, b, b), or None for zero."""
+
+    retarded: tuple | None = None
+    lesser: tuple | None = None
+    greater: tuple | None = None
+
+
+@dataclass
 class PointResult:
     transmission: torch.Tensor  # (B,) float64
     density: torch.Tensor  # (B, N*b) float64
@@ -153,6 +166,8 @@ class EnergyPointSolver:
         self._ws = WorkspacePool()
         self._grid = None  # (energies, f_left, f_right) on the device, see bind_grid
         self._cache = None  # resident surface Green's functions, see enable_obc_cache
+        self._scatt = None  # scattering self-energies of the current eager call
+        self._h_off = None
         self.lib = _native.load()
 
     # ------------------------------------------------------------------
@@ -242,10 +257,26 @@ class EnergyPointSolver:
         return QtxBT(n, bs, d, u, lo)
 
     # ------------------------------------------------------------------
-    def solve(self, energies, f_left, f_right) -> PointResult:
-        """Solves one batch of energies; all results stay on the device."""
+    def solve(self, energies, f_left, f_right, scattering: ScatteringSelfEnergy | None = None) -> PointResult:
+        """Solves one batch of energies; all results stay on the device.
+
+        ``scattering``: scattering self-energies of the batch (an SCBA
+        iteration). The system matrix is then assembled in one pass per block
+        as A = (E + i eta) I - V - H - Sigma^R - (Sigma^> - Sigma^<) / 2
+        (``qtx_assemble_system``, electron/solver.py:611-709), the boundary
+        conditions are taken from the assembled boundary blocks, and
+        Sigma^<, Sigma^> enter the selected solve (solver.py:845-872).
+        FP64 and emulated precisions; eager calls only (not captured)."""
         B = self.set_inputs(energies, f_left, f_right)
-        res = self._run(B, device_loop=self.device_loop)
+        if scattering is not None:
+            if self.precision == "mixed":
+                raise NotImplementedError("scattering self-energies are taken by the fp64 and emulated paths")
+            self._check_scattering(scattering, B)
+        self._scatt = scattering
+        try:
+            res = self._run(B, device_loop=self.device_loop)
+        finally:
+            self._scatt = None
         if not self.device_loop:
             it, conv = self._host_sr
             if not conv:
@@ -305,6 +336,44 @@ class EnergyPointSolver:
         g.replay()
         return self._result(B)
 
+    def _check_scattering(self, sc: ScatteringSelfEnergy, B: int) -> None:
+        N, b = self.N, self.b
+        for name in ("retarded", "lesser", "greater"):
+            t = getattr(sc, name)
+            if t is None:
+                continue
+            shapes = ((N, B, b, b), (N - 1, B, b, b), (N - 1, B, b, b))
+            if len(t) != 3 or any(tuple(x.shape) != sh or x.dtype != _C128 or x.device != self.device
+                                  or not x.is_contiguous() for x, sh in zip(t, shapes)):
+                raise ValueError(f"scattering.{name} must be contiguous complex128 device stacks of shapes "
+                                 f"{shapes}")
+
+    def _assembled(self, B: int, buf: dict, keep: list, stream):
+        """A(E) with the scattering self-energies: diagonal blocks into
+        a_diag, off-diagonal blocks into per-energy stacks."""
+        N, b, lib = self.N, self.b, self.lib
+        if buf.get("a_up") is None or buf["a_up"].shape[1] != B:
+            n1 = max(N - 1, 1)
+            buf["a_up"] = torch.empty((n1, B, b, b), dtype=_C128, device=self.device)
+            buf["a_lo"] = torch.empty((n1, B, b, b), dtype=_C128, device=self.device)
+        if getattr(self, "_h_off", None) is None:
+            self._h_off = ((-self.upper).contiguous(), (-self.lower).contiguous())  # H_{i,i+1}, H_{i+1,i}
+        H = self._bt([_bcast(self.h[i]) for i in range(N)], [_bcast(self._h_off[0])] * (N - 1),
+                     [_bcast(self._h_off[1])] * (N - 1), keep)
+        A = self._bt([mat(buf["a_diag"][i]) for i in range(N)], [mat(buf["a_up"][i]) for i in range(N - 1)],
+                     [mat(buf["a_lo"][i]) for i in range(N - 1)], keep)
+
+        def bt(t):
+            if t is None:
+                return None
+            return ctypes.byref(self._bt([mat(t[0][i]) for i in range(N)], [mat(t[1][i]) for i in range(N - 1)],
+                                         [mat(t[2][i]) for i in range(N - 1)], keep))
+
+        sc = self._scatt
+        _native.check(lib.qtx_assemble_system(ctypes.byref(H), None, buf["zE"].data_ptr(), bt(sc.retarded),
+                                              bt(sc.lesser), bt(sc.greater), ctypes.byref(A), B, stream))
+        return mat(buf["a_up"][0]), mat(buf["a_lo"][0]), mat(buf["a_up"][N - 2]), mat(buf["a_lo"][N - 2])
+
     def sr_status(self, B: int) -> tuple[int, bool]:
         """(decimation steps, converged) of the last device-loop run."""
         buf = self._buffers(B)
@@ -343,18 +412,23 @@ class EnergyPointSolver:
         _native.check(lib.qtx_assemble_energies(B, buf["E"].data_ptr(), float(self.eta), buf["zE"].data_ptr(),
                                                 stream))
 
-        # 1. A(E) diagonal blocks.
+        # 1. A(E): diagonal blocks (energy-independent couplings stay shared),
+        #    or every block when scattering self-energies are given.
         a_diag = buf["a_diag"]
-        for i in range(N):
-            _native.check(lib.qtx_assemble_diag(b, B, _bcast(self.h[i]), buf["zE"].data_ptr(),
-                                                mat(a_diag[i]), stream))
+        scatt = getattr(self, "_scatt", None)
+        if scatt is None:
+            for i in range(N):
+                _native.check(lib.qtx_assemble_diag(b, B, _bcast(self.h[i]), buf["zE"].data_ptr(),
+                                                    mat(a_diag[i]), stream))
+            up0, lo0 = up_n, lo_n = _bcast(self.upper), _bcast(self.lower)
+        else:
+            up0, lo0, up_n, lo_n = self._assembled(B, buf, keep, stream)
 
         # 2. Boundary conditions, left = (A00, A01, A10), right =
         #    (A_NN, A_N,N-1, A_N-1,N).
-        up, lo = _bcast(self.upper), _bcast(self.lower)
         sig = buf["sig"]
-        sides = ((a_diag[0], up, lo, buf["gl"], fl, sig[0:3]),
-                 (a_diag[N - 1], lo, up, buf["gr"], fr, sig[3:6]))
+        sides = ((a_diag[0], up0, lo0, buf["gl"], fl, sig[0:3]),
+                 (a_diag[N - 1], lo_n, up_n, buf["gr"], fr, sig[3:6]))
         if warm:
             if self._cache is None:
                 raise RuntimeError("a warm run needs enable_obc_cache()")
@@ -389,10 +463,23 @@ class EnergyPointSolver:
             up_s, lo_s, zero = _bcast(self.upper64), _bcast(self.lower64), self.zero64
         else:
             ad, sgx = a_diag, sig
-            up_s, lo_s, zero = up, lo, self.zero
-        A = self._bt([mat(ad[i]) for i in range(N)], [up_s] * (N - 1), [lo_s] * (N - 1), keep)
+            up_s, lo_s, zero = _bcast(self.upper), _bcast(self.lower), self.zero
+        if scatt is None:
+            A = self._bt([mat(ad[i]) for i in range(N)], [up_s] * (N - 1), [lo_s] * (N - 1), keep)
+        else:
+            A = self._bt([mat(ad[i]) for i in range(N)], [mat(buf["a_up"][i]) for i in range(N - 1)],
+                         [mat(buf["a_lo"][i]) for i in range(N - 1)], keep)
         zs = NULL_MAT if self.skip_zero_scattering else _bcast(zero)
         S = self._bt([zs] * N, [zs] * (N - 1), [zs] * (N - 1), keep)
+
+        def scatt_bt(t):
+            if t is None:
+                return S
+            return self._bt([mat(t[0][i]) for i in range(N)], [mat(t[1][i]) for i in range(N - 1)],
+                            [mat(t[2][i]) for i in range(N - 1)], keep)
+
+        SL = scatt_bt(scatt.lesser) if scatt is not None else S
+        SG = scatt_bt(scatt.greater) if scatt is not None else S
         if self.store_blocks:
             XL = self._bt([mat(buf["xl_d"][i]) for i in range(N)], [mat(buf["xl_u"][i]) for i in range(N - 1)],
                           [mat(buf["xl_l"][i]) for i in range(N - 1)], keep)
@@ -415,7 +502,7 @@ class EnergyPointSolver:
         with gemm_path(self.slices):
             ws = self._ws.get(wsq(N, A.block_sizes, B, 1), dev, "rgf")
             _native.check(solve(
-                ctypes.byref(A), ctypes.byref(S), ctypes.byref(S), obc[0], obc[1], obc[2], ctypes.byref(XL),
+                ctypes.byref(A), ctypes.byref(SL), ctypes.byref(SG), obc[0], obc[1], obc[2], ctypes.byref(XL),
                 ctypes.byref(XG), ctypes.byref(XR), buf["current"].data_ptr(), mat(buf["g0n"]),
                 buf["density"].data_ptr(), 0, B, buf["info"].data_ptr(), ws.data_ptr(), ws.numel(), stream))
 
