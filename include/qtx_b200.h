@@ -289,6 +289,29 @@ int qtx_beyn_moments(int n, int64_t batch, qtx_mat a_ji, qtx_mat a_ii, qtx_mat a
                      double r_i, int num_quad_points, qtx_mat q0, qtx_mat q1, int* info,
                      void* workspace, size_t workspace_bytes, qtx_stream stream);
 
+/* Workspace bytes sufficient for qtx_lyapunov_doubling and
+ * qtx_lyapunov_refine on n x n blocks. */
+size_t qtx_lyapunov_workspace(int n, int64_t batch);
+
+/* Discrete-time Lyapunov equation X = Q + A X A^H by doubling,
+ * qttools boundary_conditions/lyapunov/doubling.py:36-91 (Doubling.__call__):
+ * X_{k+1} = X_k + A_k X_k A_k^H, A_{k+1} = A_k A_k, stopped when every entry
+ * has ||X_{k+1} - X_k||_F / ||X_{k+1}||_F < rel_tol or
+ * ||X_{k+1} - X_k||_F < abs_tol. iterations / converged: host ints.
+ * Synchronises the stream once per step to test the stop rule. */
+int qtx_lyapunov_doubling(int n, int64_t batch, qtx_mat a, qtx_mat q, qtx_mat x, int max_iterations,
+                          double rel_tol, double abs_tol, int* iterations, int* converged,
+                          void* workspace, size_t workspace_bytes, qtx_stream stream);
+
+/* One fixed-point step of the Lyapunov equation with residuals,
+ * qttools boundary_conditions/lyapunov/lyapunov.py:488-579
+ * (LyapunovSystem._fixed_point_step / _get_residuals):
+ * x_ref = q + a x a^H, abs_res = ||x_ref - x||_F, rel_res = abs_res /
+ * ||x_ref||_F (device double[batch]). x_ref may equal x. */
+int qtx_lyapunov_refine(int n, int64_t batch, qtx_mat a, qtx_mat q, qtx_mat x, qtx_mat x_ref,
+                        double* rel_res, double* abs_res, void* workspace, size_t workspace_bytes,
+                        qtx_stream stream);
+
 /* Workspace bytes sufficient for qtx_contact_self_energy, qtx_obc_refine
  * and qtx_transmission (square n x n blocks) on `batch` entries. */
 size_t qtx_obc_workspace(int n, int64_t batch);

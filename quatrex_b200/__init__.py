@@ -22,11 +22,12 @@ from .obc import (OBCSolver, OBCSystem, SanchoRubio, contact_self_energy, fixed_
                   transmission)
 from .observables import density
 from .spectral import Beyn, Spectral
+from .lyapunov import Doubling, LyapunovSolver, LyapunovSystem, screened_contact_obc
 
 __all__ = [
     "DSDBCOO", "RGF", "GFSolver", "OBCBlocks", "EnergyPointSolver", "ScatteringSelfEnergy", "flops_per_energy", "OBCSolver",
     "OBCSystem", "SanchoRubio", "contact_self_energy", "fixed_point_refine", "inverse", "transmission",
-    "density", "Beyn", "Spectral",
+    "density", "Beyn", "Spectral", "Doubling", "LyapunovSolver", "LyapunovSystem", "screened_contact_obc",
 ]
 
 __version__ = "0.1.0"

@@ -105,6 +105,11 @@ SIGNATURES = {
     "qtx_beyn_moments_workspace": (c_size_t, [c_int, c_int64, c_int]),
     "qtx_beyn_moments": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, c_double, c_double, c_int, QtxMat, QtxMat,
                                  c_void_p, c_void_p, c_size_t, c_void_p]),
+    "qtx_lyapunov_workspace": (c_size_t, [c_int, c_int64]),
+    "qtx_lyapunov_doubling": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, c_int, c_double, c_double,
+                                      POINTER(c_int), POINTER(c_int), c_void_p, c_size_t, c_void_p]),
+    "qtx_lyapunov_refine": (c_int, [c_int, c_int64, QtxMat, QtxMat, QtxMat, QtxMat, c_void_p, c_void_p,
+                                    c_void_p, c_size_t, c_void_p]),
     "qtx_copy_ranges": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int64, POINTER(c_int64),
                                 POINTER(c_int64), c_int, c_void_p]),
     "qtx_profile_enable": (c_int, [c_int]),

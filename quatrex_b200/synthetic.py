@@ -217,3 +217,39 @@ def strip_lead(width: int, slices: int, energies, seed: int = 0, eta: float = ET
     a_ij = np.broadcast_to(-t, (e.size, b, b)).copy()
     a_ji = np.broadcast_to(-t.conj().T, (e.size, b, b)).copy()
     return a_ii, a_ij, a_ji
+
+
+def screened_lead(block_size: int, num_energies: int, seed: int = 0):
+    """Boundary blocks of a synthetic screened-interaction (W) problem: the
+    Coulomb matrix V (Hermitian, positive definite diagonal block, weak
+    coupling) and the retarded, lesser and greater polarization P^R, P^<,
+    P^> of ``num_energies`` energies, with the symmetries the reference
+    relies on (P^< = i X, P^> = -i Y with X, Y positive semidefinite
+    block-tridiagonal; P^R with a dissipative anti-Hermitian part).
+    Returns dicts of (x_10, x_00, x_01) triples: ``v`` of (b, b) blocks and
+    ``p_retarded``, ``p_lesser``, ``p_greater`` of (E, b, b) stacks."""
+    rng = np.random.default_rng(seed)
+    b, ne = int(block_size), int(num_energies)
+
+    def cplx(*s):
+        return rng.standard_normal(s) + 1j * rng.standard_normal(s)
+
+    def h(x):
+        return x.conj().swapaxes(-2, -1)
+
+    u, _ = np.linalg.qr(cplx(b, b))
+    v00 = (u * rng.uniform(0.2, 1.0, b)) @ h(u) * 0.5
+    v01 = 0.05 * cplx(b, b)
+    v = (h(v01), v00, v01)
+    herm = 0.5 * (cplx(ne, b, b) + h(cplx(ne, b, b)))
+    g = cplx(ne, b, b)
+    p00 = 0.04 * herm - 0.02j * (g @ h(g)) / b
+    p01 = 0.01 * cplx(ne, b, b)
+    p10 = 0.01 * cplx(ne, b, b)
+    out = {"v": v, "p_retarded": (p10, p00, p01)}
+    for name, sign in (("p_lesser", 1.0), ("p_greater", -1.0)):
+        q0, q1 = cplx(ne, b, b) * 0.1, cplx(ne, b, b) * 0.05
+        x00 = q0 @ h(q0) + q1 @ h(q1)
+        x01 = q1 @ h(q0)
+        out[name] = (1j * sign * h(x01), 1j * sign * x00, 1j * sign * x01)
+    return out
