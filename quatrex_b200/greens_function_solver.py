@@ -216,10 +216,10 @@ class RGF(GFSolver):
                                   slices, out, return_retarded, return_current):
         """selected_solve for host (CPU torch) containers with more than one
         batch: uploads run on a copy stream two batches ahead and write-backs
-        on a third stream while a batch is solved. The first and the last
-        batch are split in halves so that the upload before the first solve
-        and the write-back after the last one (the parts nothing overlaps)
-        are short. The copy streams persist across calls, so the caching
+        on a third stream while a batch is solved. The batches are shifted
+        by half a batch so that the first and the last are half as large:
+        the upload before the first solve and the write-back after the last
+        one (the parts nothing overlaps) are short. The copy streams persist across calls, so the caching
         allocator reuses their buffers instead of allocating new ones each
         call. Same results and conventions; a singular block raises after the
         last batch."""
@@ -410,15 +410,23 @@ def _copy_streams(device: torch.device):
 
 
 def _split_ends(slices) -> np.ndarray:
-    """Batch boundaries with the first and the last batch halved."""
+    """Pipeline batch boundaries: the reference's batches shifted by half a
+    batch, so that the first and the last pipeline batch are half as large
+    (short upload before the first solve and write-back after the last one)
+    and every other batch keeps the full size (no batch exceeds the
+    caller's max_batch_size)."""
     b = [int(x) for x in slices]
-    if len(b) >= 3:  # at least two batches
-        first, last = b[1] - b[0], b[-1] - b[-2]
-        if last >= 2:
-            b.insert(len(b) - 1, b[-2] + last // 2)
-        if first >= 2:
-            b.insert(1, b[0] + first // 2)
-    return np.asarray(b)
+    if len(b) < 3:  # a single batch: nothing to overlap
+        return np.asarray(b)
+    size = max(b[i + 1] - b[i] for i in range(len(b) - 1))
+    half = max(size // 2, 1)
+    total = b[-1]
+    out = [0, half]
+    while out[-1] + size < total:
+        out.append(out[-1] + size)
+    if out[-1] < total:
+        out.append(total)
+    return np.asarray(out)
 
 
 def _on_host(m) -> bool:
