@@ -77,8 +77,9 @@ def parse():
                    help="arrival rate as a fraction of the capacity measured per lane")
     p.add_argument("--graph", action="store_true",
                    help="replay each batch through one captured CUDA graph (device-side Sancho-Rubio loop)")
-    p.add_argument("--inverse-path", choices=["auto", "single", "wide", "cluster"], default="auto",
-                   help="inverse kernels: automatic choice, one CTA per matrix, or multi-CTA panels")
+    p.add_argument("--inverse-path", choices=["auto", "single", "wide", "cluster", "split"], default="auto",
+                   help="inverse kernels: automatic choice, one CTA per matrix, multi-CTA panels, one "
+                        "thread-block cluster per matrix, or the one-CTA kernel column-split over a cluster")
     return p.parse_args()
 
 
@@ -1084,7 +1085,7 @@ def run_kernels(args, local):
     info = torch.zeros(B, dtype=torch.int32, device=device)
     ws = torch.empty(lib.qtx_zinv_workspace(n, B), dtype=torch.uint8, device=device)
     for name, mode in (("zinv_ours_one_cta_per_matrix", 1), ("zinv_ours_multi_cta", 2),
-                       ("zinv_ours_cluster", 3)):
+                       ("zinv_ours_cluster", 3), ("zinv_ours_column_split", 4), ("zinv_ours_automatic", 0)):
         _native.check(lib.qtx_set_inverse_path(mode))
         out[name] = flops / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
             n, B, mat(w), mat(c), info.data_ptr(), ws.data_ptr(), ws.numel(), stream()))) / 1e12
@@ -1101,8 +1102,9 @@ def run_kernels(args, local):
             cn = torch.empty_like(wn)
             wsn = torch.empty(lib.qtx_zinv_workspace(nn, nb), dtype=torch.uint8, device=device)
             row = {}
-            for name, mode in (("one_cta", 1), ("multi_cta", 2), ("cluster", 3)):
-                if mode == 3 and nn > 256:
+            for name, mode in (("one_cta", 1), ("multi_cta", 2), ("cluster", 3), ("column_split", 4),
+                               ("automatic", 0)):
+                if (mode == 3 and nn > 256) or (mode == 4 and nn > 400):
                     continue
                 _native.check(lib.qtx_set_inverse_path(mode))
                 row[name] = 8.0 * nn ** 3 * nb / timeit(lambda: _native.check(lib.qtx_zinv_batched_ws(
@@ -1126,7 +1128,7 @@ def main():
         return
     from quatrex_b200 import _native
 
-    _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2, "cluster": 3}[args.inverse_path]))
+    _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2, "cluster": 3, "split": 4}[args.inverse_path]))
     if args.workload != "cfg1":
         if rank == 0:
             {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels}[args.workload](args, local)

@@ -140,12 +140,18 @@ int qtx_zinv_batched_ws(int n, int64_t batch, qtx_mat a, qtx_mat x, int* info, v
                         size_t workspace_bytes, qtx_stream stream);
 
 /* Inverse path of every inverse in this process: 0 automatic (default),
- * 1 one CTA per matrix, 2 multi-CTA (workspace-backed calls), 3 one
- * thread-block cluster of ceil(n / 32) CTAs per matrix holding it in
- * distributed shared memory (n <= 256; loaded with TMA). Automatic picks the
- * cluster kernel for n <= 256 while batch x ceil(n / 32) is at most half the
- * SM count (the small batches where one matrix's latency dominates). A
- * tuning and test knob; no reference counterpart. */
+ * 1 one CTA per matrix, 2 multi-CTA (workspace-backed calls, n > 400 in the
+ * automatic choice), 3 one thread-block cluster of ceil(n / 32) CTAs per
+ * matrix holding it in distributed shared memory (n <= 256; loaded with
+ * TMA), 4 the one-CTA kernel as a cluster of C CTAs per matrix that split
+ * its columns (n <= 400; C the largest of 2, 4, 8 leaving 32 columns per
+ * CTA). Automatic: the distributed-shared-memory cluster for n <= 256 while
+ * batch x ceil(n / 32) is at most half the SM count; else up to n = 400 the
+ * column split with the largest C for which batch x C fits the SM count and
+ * every cluster is co-resident (C = 1 at full batches); above n = 400 the
+ * multi-CTA path for batches up to half the SM count. All paths use the same
+ * pivot rule; paths 1 and 4 give bit-identical results. A tuning and test
+ * knob; no reference counterpart. */
 int qtx_set_inverse_path(int mode);
 /* 1 if a bounded wait inside the cluster inverse timed out since the last
  * call (the flag is cleared; those results are invalid), 0 if not, < 0 on

@@ -301,8 +301,8 @@ int qtx_inverse_status(void) {
 }
 
 int qtx_set_inverse_path(int mode) {
-  if (mode < 0 || mode > 3) {
-    set_error("qtx_set_inverse_path: mode must be 0, 1, 2 or 3");
+  if (mode < 0 || mode > 4) {
+    set_error("qtx_set_inverse_path: mode must be 0, 1, 2, 3 or 4");
     return QTX_ERR_ARG;
   }
   set_inverse_path(mode);

@@ -158,6 +158,8 @@ int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* acti
             size_t scratch_bytes, cudaStream_t s);
 bool zinv_prefers_wide(int n, int64_t batch);
 void set_inverse_path(int mode);
+int inverse_path();
+int num_sms();
 // One thread-block cluster of ceil(n / 32) CTAs per matrix with the matrix in
 // distributed shared memory (zinv_cluster.cu); n <= 256, no scratch.
 int zinv_cluster(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s);

@@ -8,12 +8,19 @@
 // connected Green's functions g_i stay resident in a caller-provided
 // workspace; results go straight to the caller's output block views.
 //
+// In the forward sweep of selected_solve the retarded chain (Schur
+// complement, inverse) runs on a high-priority helper stream while the
+// lesser/greater products of the previous block run on the caller's stream:
+// at small batches the inverse is latency-bound on a few SMs and the
+// products fill the rest of the GPU beside it.
+//
 // Products that the reference evaluates twice are evaluated once (e.g.
 // x_ii @ a_ij in rgf.py:107,110 and xr_ii @ sigma_ij in rgf.py:346,354), and
 // the Meir-Wingreen current reuses the forward-sweep Sigma-tilde instead of
 // recomputing it (rgf.py:388-402 repeats rgf.py:272-301): the same
 // algebra with fewer products.
 #include <algorithm>
+#include <map>
 #include <vector>
 
 #include "common.cuh"
@@ -268,6 +275,32 @@ int copy_block_t(int m, int n, int64_t batch, MatRef dst, MatRef src, cudaStream
   return P::combine(m, n, batch, dst, &t, 1, s);
 }
 
+// A helper stream per (device, caller stream) of the calling thread, at the
+// device's highest priority, with the events that order it against the
+// caller's stream; created on first use, kept for the thread's lifetime.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, inv = nullptr, xdone[2] = {nullptr, nullptr};
+};
+
+int side_stream(cudaStream_t s, SideStream** out) {
+  thread_local std::map<std::pair<int, cudaStream_t>, SideStream> reg;
+  int dev = 0;
+  QTX_CHECK_CUDA(cudaGetDevice(&dev));
+  SideStream& e = reg[{dev, s}];
+  if (e.s == nullptr) {
+    int least = 0, greatest = 0;
+    QTX_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    QTX_CHECK_CUDA(cudaEventCreateWithFlags(&e.fork, cudaEventDisableTiming));
+    QTX_CHECK_CUDA(cudaEventCreateWithFlags(&e.inv, cudaEventDisableTiming));
+    QTX_CHECK_CUDA(cudaEventCreateWithFlags(&e.xdone[0], cudaEventDisableTiming));
+    QTX_CHECK_CUDA(cudaEventCreateWithFlags(&e.xdone[1], cudaEventDisableTiming));
+    QTX_CHECK_CUDA(cudaStreamCreateWithPriority(&e.s, cudaStreamNonBlocking, greatest));
+  }
+  *out = &e;
+  return QTX_OK;
+}
+
 }  // namespace
 
 template <class Prec>
@@ -289,7 +322,7 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
       st[x].resize(N);
       for (int i = 0; i < N; ++i) st[x][i] = ws.mat(bs[i], bs[i], batch, Prec::E);
     }
-  enum { P_, M_, T_, Q_, T2_, U_, V_, W_, Z_, R1_, TT_, T1X_, T2X_, Y_, XIJ_, GA_, GB_, CA_, CB_, NT_ };
+  enum { P_, P2_, M_, T_, Q_, T2_, U_, V_, W_, Z_, R1_, TT_, T1X_, T2X_, Y_, XIJ_, GA_, GB_, CA_, CB_, NT_ };
   MatRef tmp[NT_];
   for (int k = 0; k < NT_; ++k) tmp[k] = ws.mat(bm, bm, batch, Prec::E);
   MatRef inv_tmp = Prec::kInvTmp ? ws.mat(bm, bm, batch, sizeof(z64)) : MatRef{};
@@ -330,16 +363,34 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
       QTX_TRY(Gemm(bs[0], bs[0], bs[0], batch, T2, 0, gR[0], 1, gX[x][0]).run(s));
     }
   }
-  // Forward sweep (rgf.py:241-302).
+  // Forward sweep (rgf.py:241-302). The retarded chain runs on the helper
+  // stream `sr`; the lesser/greater products of block j wait for the inverse
+  // of block j, and the helper reuses the buffer of P (double-buffered by the
+  // parity of j) only after the products of block j - 2 are done. Not with
+  // the int8-emulated products, whose digit-plane scratch is shared.
+  const bool use_side = N > 1 && !(gemm_slices() > 0 && oz_bound(nullptr) != nullptr);
+  SideStream* ss = nullptr;
+  cudaStream_t sr = s;
+  if (use_side) {
+    QTX_TRY(side_stream(s, &ss));
+    sr = ss->s;
+    QTX_CHECK_CUDA(cudaEventRecord(ss->fork, s));
+    QTX_CHECK_CUDA(cudaStreamWaitEvent(sr, ss->fork, 0));
+  }
   for (int j = 1; j < N; ++j) {
     const int i = j - 1;
-    MatRef P = shaped(tmp[P_], bs[i]);
-    QTX_TRY(Gemm(bs[j], bs[i], bs[i], batch, a.lower[i], 0, gR[i], 0, P).run(s));
+    MatRef P = shaped(tmp[(j & 1) ? P2_ : P_], bs[i]);
+    if (use_side && j >= 3) QTX_CHECK_CUDA(cudaStreamWaitEvent(sr, ss->xdone[j & 1], 0));
+    QTX_TRY(Gemm(bs[j], bs[i], bs[i], batch, a.lower[i], 0, gR[i], 0, P).run(sr));
     QTX_TRY(Gemm(bs[j], bs[j], bs[i], batch, P, 0, a.upper[i], 0, gR[j], MONE)
                 .plus(a.diag[j], ONE)
                 .plus(obc(io.obc_r, j), MONE)
-                .run(s));
-    QTX_TRY(Prec::inv(bs[j], batch, gR[j], info, inv_tmp, inv_scr, inv_scr_bytes, s));
+                .run(sr));
+    QTX_TRY(Prec::inv(bs[j], batch, gR[j], info, inv_tmp, inv_scr, inv_scr_bytes, sr));
+    if (use_side) {
+      QTX_CHECK_CUDA(cudaEventRecord(ss->inv, sr));
+      QTX_CHECK_CUDA(cudaStreamWaitEvent(s, ss->inv, 0));
+    }
     for (int x = 0; x < 2; ++x) {
       MatRef Q{};
       if (!supper(x, i).null()) {
@@ -370,7 +421,10 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
       QTX_TRY(Gemm(bs[j], bs[j], bs[j], batch, gR[j], 0, M, 0, T2).run(s));
       QTX_TRY(Gemm(bs[j], bs[j], bs[j], batch, T2, 0, gR[j], 1, gX[x][j]).run(s));
     }
+    if (use_side) QTX_CHECK_CUDA(cudaEventRecord(ss->xdone[j & 1], s));
   }
+  // (The caller's stream has waited for the last inverse: every helper-stream
+  // launch is ordered before what follows.)
   // Last diagonal blocks (rgf.py:305-312).
   for (int x = 0; x < 2; ++x)
     QTX_TRY(Prec::antiherm(bs[N - 1], batch, gX[x][N - 1], odiag(x, N - 1),

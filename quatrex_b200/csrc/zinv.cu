@@ -21,8 +21,12 @@
 //     5. write the panel back.
 //   Finally undo the column permutation (pivots applied in reverse order).
 // Total work n^3 complex multiply-adds = 8 n^3 real flops.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "gj_panel.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace qtx {
 namespace {
@@ -391,9 +395,18 @@ struct Smem2 {
   }
 };
 
+// Column split (csplit = C > 1, launched as clusters of C CTAs, one matrix
+// per cluster): every CTA of the cluster factors each panel itself (the
+// same arithmetic on the same data, so the same transform and pivots) and
+// applies it to its own range of whole panels' columns; the panel's columns
+// are written back by the CTA that owns them. A cluster barrier after each
+// panel orders the owner's writes before the next panel's loads (read
+// through L2), and the final row gather is split by rows. The serial panel
+// factorization stays, the update is divided by C: for small batches, C SMs
+// per matrix instead of one.
 template <int NB>
 __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatRef A, MatRef X, int* info,
-                                                      const int* active) {
+                                                      const int* active, int csplit) {
   using S = Smem2<NB>;
   // Column block of the row-interchange pass: all 2 NB affected rows of CW
   // columns fit T2 x PV registers.
@@ -416,20 +429,31 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
+  const int rank = (int)(blockIdx.x % csplit);
+  // this CTA's columns [c_lo, c_hi): whole panels
+  auto cbound = [&](int q) {
+    const int v = (int)(((int64_t)n * q / csplit + NB - 1) / NB) * NB;
+    return v < n ? v : n;
+  };
+  const int c_lo = cbound(rank), c_hi = cbound(rank + 1), cw = c_hi - c_lo;
+  auto cluster_sync = [&]() {
+    if (csplit > 1) cg::this_cluster().sync();
+  };
 
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+  for (int64_t b = blockIdx.x / csplit; b < batch; b += gridDim.x / csplit) {
     if (active != nullptr && active[b] == 0) continue;
     const z64* a = at<const z64>(A, b);
     z64* x = at<z64>(X, b);
     const int64_t ldx = X.ld;
     if (a != x) {
-      for (int64_t idx = tid; idx < (int64_t)n * n; idx += T2) {
-        const int r = (int)(idx / n), c = (int)(idx % n);
+      for (int64_t idx = tid; idx < (int64_t)n * cw; idx += T2) {
+        const int r = (int)(idx / cw), c = c_lo + (int)(idx % cw);
         x[(int64_t)r * ldx + c] = a[(int64_t)r * A.ld + c];
       }
     }
     if (tid == 0) s_sing = 0;
     __syncthreads();
+    cluster_sync();
 
     for (int k0 = 0; k0 < n; k0 += NB) {
       const int nbp = min(NB, n - k0);
@@ -439,7 +463,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
       if (NB == 16 && n <= 256) {
       for (int idx = tid; idx < n * NB; idx += T2) {
         const int r = idx / NB, c = idx % NB;
-        P[r * PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
+        P[r * PS + c] = (c < nbp) ? __ldcg(&x[(int64_t)r * ldx + k0 + c]) : make_double2(0.0, 0.0);
       }
       __syncthreads();
       gj_factor_panel16(
@@ -449,7 +473,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
       } else {
       for (int idx = tid; idx < n * NB; idx += T2) {
         const int r = idx / NB, c = idx % NB;
-        P[r * PS + c] = (c < nbp) ? x[(int64_t)r * ldx + k0 + c] : make_double2(0.0, 0.0);
+        P[r * PS + c] = (c < nbp) ? __ldcg(&x[(int64_t)r * ldx + k0 + c]) : make_double2(0.0, 0.0);
       }
       __syncthreads();
       double best = -1.0;
@@ -556,7 +580,8 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
       }
       __syncthreads();
       const int na = s_na;
-      const int oc = n - nbp;  // columns outside the panel
+      const bool pin = k0 >= c_lo && k0 < c_hi;  // the panel lies in this CTA's columns
+      const int oc = cw - (pin ? nbp : 0);       // this CTA's columns outside the panel
       // In column blocks of CW: all affected rows of a column move within
       // one block (read all, barrier, write all).
       for (int cb = 0; cb < oc; cb += CW) {
@@ -566,7 +591,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
           const int li = tid + u * T2;
           const int aa = li / CW, cc = cb + li % CW;
           if (aa < na && cc < oc) {
-            const int c = cc < k0 ? cc : cc + nbp;
+            const int c = c_lo + cc + ((pin && c_lo + cc >= k0) ? nbp : 0);
             v[u] = x[(int64_t)aff_src[aa] * ldx + c];
           }
         }
@@ -576,7 +601,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
           const int li = tid + u * T2;
           const int aa = li / CW, cc = cb + li % CW;
           if (aa < na && cc < oc) {
-            const int c = cc < k0 ? cc : cc + nbp;
+            const int c = c_lo + cc + ((pin && c_lo + cc >= k0) ? nbp : 0);
             x[(int64_t)aff_row[aa] * ldx + c] = v[u];
           }
         }
@@ -586,8 +611,9 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
       const int ny = YS - 2;  // columns of whole tiles; those >= n stay zero
       for (int idx = tid; idx < NB * ny; idx += T2) {
         const int kk = idx / ny, c = idx % ny;
-        Y[kk * YS + c] = (kk < nbp && c < n && (c < k0 || c >= k0 + nbp)) ? x[(int64_t)(k0 + kk) * ldx + c]
-                                                                          : make_double2(0.0, 0.0);
+        Y[kk * YS + c] = (kk < nbp && c >= c_lo && c < c_hi && (c < k0 || c >= k0 + nbp))
+                             ? x[(int64_t)(k0 + kk) * ldx + c]
+                             : make_double2(0.0, 0.0);
       }
       __syncthreads();
       // 4. Trailing update, one 16-row slice per warp at a time, no barriers.
@@ -595,7 +621,7 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
       for (int mt = warp; mt < mtiles; mt += W2) {
         const int r0 = mt * 16;
         // A fragments of this slice for all k (the panel transform rows).
-        for (int j0 = 0; j0 < n; j0 += 8 * JN) {
+        for (int j0 = c_lo; j0 < c_hi; j0 += 8 * JN) {
           if (j0 >= k0 && j0 + 8 * JN <= k0 + nbp) continue;  // inside the panel
           double cre[JN][4], cim[JN][4];
 #pragma unroll
@@ -646,12 +672,15 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
         }
       }
       __syncthreads();
-      // 5. The panel transform back into X[:, K].
-      for (int idx = tid; idx < n * nbp; idx += T2) {
-        const int r = idx / nbp, c = idx % nbp;
-        x[(int64_t)r * ldx + k0 + c] = P[r * PS + c];
+      // 5. The panel transform back into X[:, K] (by the CTA owning K).
+      if (pin) {
+        for (int idx = tid; idx < n * nbp; idx += T2) {
+          const int r = idx / nbp, c = idx % nbp;
+          x[(int64_t)r * ldx + k0 + c] = P[r * PS + c];
+        }
       }
       __syncthreads();
+      cluster_sync();
     }
 
     // Undo the column permutation: swaps applied from the last pivot back.
@@ -668,23 +697,28 @@ __global__ void __launch_bounds__(T2, 1) zinv2_kernel(int n, int64_t batch, MatR
     }
     __syncthreads();
     // Row-wise gather through the (now free) panel buffer: PS rows fit.
+    // Rows rank, rank + C, ... of a column split (read through L2: the
+    // other CTAs wrote their columns).
     const int nbufs = PS < W2 ? PS : W2;
     if (warp < nbufs) {
       z64* rowbuf = P + (size_t)warp * n;
-      for (int r = warp; r < n; r += nbufs) {
-        for (int c = lane; c < n; c += 32) rowbuf[c] = x[(int64_t)r * ldx + colsrc[c]];
+      for (int r = rank + warp * csplit; r < n; r += nbufs * csplit) {
+        for (int c = lane; c < n; c += 32) rowbuf[c] = __ldcg(&x[(int64_t)r * ldx + colsrc[c]]);
         __syncwarp();
         for (int c = lane; c < n; c += 32) x[(int64_t)r * ldx + c] = rowbuf[c];
         __syncwarp();
       }
     }
-    if (tid == 0 && info != nullptr && s_sing != 0 && info[b] == 0) info[b] = s_sing;
+    if (tid == 0 && rank == 0 && info != nullptr && s_sing != 0 && info[b] == 0) info[b] = s_sing;
     __syncthreads();
+    // the next matrix's copy must not overwrite rows still being gathered
+    cluster_sync();
   }
 }
 
 template <int NB>
-int launch2(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s) {
+int launch2(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, cudaStream_t s,
+            int csplit = 1) {
   const size_t smem = Smem2<NB>::bytes(n);
   if (smem > 227 * 1024) {
     set_error("zinv: block size too large for the shared-memory panel");
@@ -692,11 +726,76 @@ int launch2(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* acti
   }
   QTX_CHECK_CUDA(
       cudaFuncSetAttribute(zinv2_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const unsigned grid = (unsigned)(batch < 1048576 ? batch : 1048576);
+  const int64_t mats = batch < 131072 ? batch : 131072;
   ProfScope prof(QTX_KERNEL_ZINV, 8.0 * (double)n * n * n * (double)batch, s);
-  zinv2_kernel<NB><<<grid, T2, smem, s>>>(n, batch, A, X, info, active);
-  QTX_CHECK_LAUNCH();
+  if (csplit <= 1) {
+    zinv2_kernel<NB><<<(unsigned)mats, T2, smem, s>>>(n, batch, A, X, info, active, 1);
+    QTX_CHECK_LAUNCH();
+    return QTX_OK;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(mats * csplit), 1, 1);
+  cfg.blockDim = dim3(T2, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)csplit;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  QTX_CHECK_CUDA(cudaLaunchKernelEx(&cfg, zinv2_kernel<NB>, n, batch, A, X, info, active, csplit));
   return QTX_OK;
+}
+
+// Column split for n <= 400 (16-column panels): the largest C in {1, 2, 4, 8}
+// with batch x C within the SM count, at least 32 columns per CTA, and all
+// batch clusters co-resident (cudaOccupancyMaxActiveClusters, cached per
+// n and C). Inverse path 4 forces the largest C the block size allows.
+int column_split(int n, int64_t batch) {
+  const int path = inverse_path();
+  if ((path != 0 && path != 4) || n > 400) return 1;
+  int cmax = 1;
+  while (cmax < 8 && n / (2 * cmax) >= 32) cmax *= 2;
+  if (path == 4) return cmax;
+  const int sms = num_sms();
+  int c = 1;
+  while (c < cmax && batch * (2 * c) <= sms) c *= 2;
+  while (c > 1) {
+    static thread_local std::vector<std::pair<int64_t, int>> cache;  // (n * 16 + c, active clusters)
+    const int64_t key = (int64_t)n * 16 + c;
+    int active = -1;
+    for (auto& e : cache)
+      if (e.first == key) active = e.second;
+    if (active < 0) {
+      const size_t smem = Smem2<16>::bytes(n);
+      if (cudaFuncSetAttribute(zinv2_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+        return 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(c * batch), 1, 1);
+      cfg.blockDim = dim3(T2, 1, 1);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)c;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, zinv2_kernel<16>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        nc = 0;
+      }
+      active = nc;
+      cache.emplace_back(key, active);
+    }
+    if (active >= batch) return c;
+    c /= 2;
+  }
+  return 1;
 }
 
 }  // namespace
@@ -708,7 +807,7 @@ int zinv(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active,
     return QTX_ERR_ARG;
   }
   if (zinv_prefers_cluster(n, batch)) return zinv_cluster(n, batch, A, X, info, active, s);
-  if (n <= 400) return launch2<16>(n, batch, A, X, info, active, s);
+  if (n <= 400) return launch2<16>(n, batch, A, X, info, active, s, column_split(n, batch));
   if (n <= 720) return launch2<8>(n, batch, A, X, info, active, s);
   if (n <= 1024) return launch<8>(n, batch, A, X, info, active, s);
   set_error("zinv: block sizes above 1024 are not supported");

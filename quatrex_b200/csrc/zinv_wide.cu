@@ -274,7 +274,9 @@ int run_wide(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* act
   return QTX_OK;
 }
 
-int g_inverse_path = 0;  // 0 automatic, 1 one CTA per matrix, 2 multi-CTA, 3 cluster
+int g_inverse_path = 0;  // 0 automatic, 1 one CTA per matrix, 2 multi-CTA, 3 cluster, 4 column split
+
+}  // namespace
 
 int num_sms() {
   static int sms = 0;
@@ -286,6 +288,10 @@ int num_sms() {
   }
   return sms;
 }
+
+int inverse_path() { return g_inverse_path; }
+
+namespace {
 
 // Panel width: as wide as the n x NB panel fits in shared memory.
 int panel_width(int n) { return n <= 416 ? 32 : (n <= 832 ? 16 : 8); }
@@ -314,14 +320,15 @@ bool zinv_prefers_cluster(int n, int64_t batch) {
 }
 
 bool zinv_prefers_wide(int n, int64_t batch) {
-  if (g_inverse_path == 1 || g_inverse_path == 3) return false;
+  if (g_inverse_path == 1 || g_inverse_path == 3 || g_inverse_path == 4) return false;
   if (g_inverse_path == 2) return true;
   // One CTA per matrix leaves SMs idle when the batch is below the SM count;
   // the multi-CTA path pays n/NB launches and a pass over the matrix per
-  // panel. Measured crossover on B200 (TFLOP/s of both paths against the
-  // batch): n = 256 up to batch 32, n = 384 and 512 up to batch 64.
+  // panel. Up to n = 400 the column-split clusters of the one-CTA kernel
+  // (zinv.cu) use the idle SMs instead; above, the measured crossover on
+  // B200 (TFLOP/s of both paths against the batch) is batch 64 at n = 512.
   const int sms = num_sms();
-  return (n >= 384 && batch * 2 <= sms) || (n >= 192 && batch * 4 <= sms);
+  return n > 400 && batch * 2 <= sms;
 }
 
 int zinv_ex(int n, int64_t batch, MatRef A, MatRef X, int* info, const int* active, void* scratch,
