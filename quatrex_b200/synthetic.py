@@ -253,3 +253,55 @@ def screened_lead(block_size: int, num_energies: int, seed: int = 0):
         x01 = q1 @ h(q0)
         out[name] = (1j * sign * h(x01), 1j * sign * x00, 1j * sign * x01)
     return out
+
+
+def screened_device(num_blocks: int, block_size: int, num_energies: int, seed: int = 0,
+                    interior: float = 0.3):
+    """Block-tridiagonal inputs of a synthetic screened-interaction (W) solve
+    in small blocks: the Coulomb matrix V (Hermitian; positive definite
+    diagonal blocks, weak coupling) and, for ``num_energies`` energies, the
+    lesser and greater polarization P^< = i X, P^> = -i Y (X, Y positive
+    semidefinite: X = Q Q^H with Q block lower bidiagonal) and the Hermitian
+    part P^R_h of the retarded polarization. The first two and the last two
+    blocks repeat one periodic lead cell (the contacts' boundary blocks);
+    the blocks in between are the lead's blocks perturbed by ``interior``
+    relative random parts. Returns a dict with ``v`` = (diag, upper, lower)
+    lists of (b, b) blocks and ``p_lesser``, ``p_greater``,
+    ``p_retarded_hermitian`` = (diag, upper, lower) lists of (E, b, b)
+    stacks (upper[i] = block (i, i+1), lower[i] = block (i+1, i))."""
+    rng = np.random.default_rng(seed)
+    n, b, ne = int(num_blocks), int(block_size), int(num_energies)
+
+    def cplx(*s):
+        return rng.standard_normal(s) + 1j * rng.standard_normal(s)
+
+    def h(x):
+        return x.conj().swapaxes(-2, -1)
+
+    def lead_or_interior(i, lead, draw):
+        # blocks 0, 1 and n-2, n-1 belong to the contacts' periodic cells
+        if i <= 1 or i >= n - 2:
+            return lead
+        return lead * (1.0 + interior * draw())
+
+    u, _ = np.linalg.qr(cplx(b, b))
+    v00 = (u * rng.uniform(0.2, 1.0, b)) @ h(u) * 0.5
+    v01 = 0.05 * cplx(b, b)
+    v_diag = [v00.copy() for _ in range(n)]
+    v_upper = [lead_or_interior(i, v01, lambda: rng.uniform()) for i in range(n - 1)]
+    v_lower = [h(x) for x in v_upper]
+    herm = 0.5 * (cplx(ne, b, b) + h(cplx(ne, b, b)))
+    p_diag = [lead_or_interior(i, 0.04 * herm, lambda: rng.uniform()) for i in range(n)]
+    p_up = 0.01 * cplx(ne, b, b)
+    p_upper = [lead_or_interior(i, p_up, lambda: rng.uniform()) for i in range(n - 1)]
+    p_lower = [h(x) for x in p_upper]
+    out = {"v": (v_diag, v_upper, v_lower), "p_retarded_hermitian": (p_diag, p_upper, p_lower)}
+    for name, sign in (("p_lesser", 1.0), ("p_greater", -1.0)):
+        q0, q1 = cplx(ne, b, b) * 0.1, cplx(ne, b, b) * 0.05
+        qd = [lead_or_interior(i, q0, lambda: rng.uniform()) for i in range(n)]
+        qs = [lead_or_interior(i, q1, lambda: rng.uniform()) for i in range(n)]  # Q[i, i-1] = qs[i]
+        xd = [qd[i] @ h(qd[i]) + qs[i] @ h(qs[i]) for i in range(n)]
+        xl = [qs[i + 1] @ h(qd[i]) for i in range(n - 1)]  # X[i+1, i]
+        xu = [h(x) for x in xl]
+        out[name] = ([1j * sign * x for x in xd], [1j * sign * x for x in xu], [1j * sign * x for x in xl])
+    return out
