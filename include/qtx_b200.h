@@ -229,6 +229,15 @@ int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
                              double* density, int flags, int64_t batch, int* info, void* workspace,
                              size_t workspace_bytes, qtx_stream stream);
 
+/* Elementwise combination out = sum_k coef_k op_k(term_k) over an m x n
+ * stack (1 to 4 terms; coefs: 2 * nterms doubles, re and im of each;
+ * conj_trans: NULL or nterms flags, 1 = conjugate transpose, m == n).
+ * out may alias a term read without transposition. The block additions of
+ * the reference's assembly steps (e.g. quatrex/coulomb_screening/
+ * solver.py:473-493, P^R = P^R_h + (P^> - P^<) / 2). */
+int qtx_zcombine(int m, int n, int64_t batch, qtx_mat out, int nterms, const qtx_mat* terms,
+                 const double* coefs, const int* conj_trans, qtx_stream stream);
+
 /* Converts an m x n stack between complex128 (QTX_C128) and complex64
  * (QTX_C64), or copies it within one type. */
 int qtx_convert(int m, int n, int64_t batch, qtx_mat in, int in_dtype, qtx_mat out, int out_dtype,

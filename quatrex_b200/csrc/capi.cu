@@ -436,6 +436,27 @@ int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
   });
 }
 
+int qtx_zcombine(int m, int n, int64_t batch, qtx_mat out, int nterms, const qtx_mat* terms,
+                 const double* coefs, const int* conj_trans, qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || batch < 0 || out.ptr == nullptr || nterms < 1 || nterms > kMaxAddends ||
+        terms == nullptr || coefs == nullptr) {
+      set_error("qtx_zcombine: invalid arguments (1 to 4 terms, non-null output)");
+      return (int)QTX_ERR_ARG;
+    }
+    Addend t[kMaxAddends];
+    for (int k = 0; k < nterms; ++k) {
+      if (terms[k].ptr == nullptr) {
+        set_error("qtx_zcombine: null term");
+        return (int)QTX_ERR_ARG;
+      }
+      t[k] = Addend{from_abi(terms[k]), make_double2(coefs[2 * k], coefs[2 * k + 1]),
+                    conj_trans ? conj_trans[k] : 0};
+    }
+    return zcombine(m, n, batch, from_abi(out), t, nterms, nullptr, (cudaStream_t)stream);
+  });
+}
+
 int qtx_convert(int m, int n, int64_t batch, qtx_mat in, int in_dtype, qtx_mat out, int out_dtype,
                 qtx_stream stream) {
   return guarded([&] {

@@ -1,0 +1,107 @@
+"""The GPU screened-interaction (W) solve against the reference's own
+``CoulombScreeningSolver.solve`` (src/quatrex/coulomb_screening/solver.py:
+724-889), recorded in ``tests/golden/w_solve.npz`` (9 small blocks of 8,
+superblocks of three, 5 energies; without and with the DOS peak filter).
+
+Tolerance: 1e-10 relative to the largest entry of each block stack (the
+FP64 selected-solve gate; every product here is a DMMA GEMM instead of
+OpenBLAS, and the boundary conditions come from the same Sancho-Rubio and
+Lyapunov doubling iterations)."""
+
+import numpy as np
+import pytest
+import torch
+
+from quatrex_b200 import DSDBCOO
+from quatrex_b200.screening import CoulombScreeningSolve
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def fixture(golden):
+    return golden("w_solve")
+
+
+def _bt(g, k):
+    return (list(g[f"{k}_diag"]), list(g[f"{k}_upper"]), list(g[f"{k}_lower"]))
+
+
+def _solver(g, device, **kw):
+    return CoulombScreeningSolve(_bt(g, "v"), int(g["num_connected_blocks"]), g["energies"], device=device, **kw)
+
+
+def _solve(g, solver):
+    return solver.solve(_bt(g, "p_lesser"), _bt(g, "p_greater"), _bt(g, "p_retarded_hermitian"))
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def _check(w, g, prefix):
+    for name, ww in zip(("wl", "wg"), w):
+        for t, part in enumerate(("diag", "upper", "lower")):
+            got = torch.stack(ww[t]).cpu().numpy()
+            ref = g[f"{prefix}_{name}_{part}"]
+            assert _rel(got, ref) < TOL, (prefix, name, part, _rel(got, ref))
+
+
+def test_w_solve_matches_reference(cuda_device, fixture):
+    g = fixture
+    w = _solve(g, _solver(g, cuda_device, filtering_iteration_limit=0))
+    _check(w, g, "plain")
+
+
+def test_w_solve_peak_filter_matches_reference(cuda_device, fixture):
+    g = fixture
+    s = _solver(g, cuda_device, dos_peak_limit=float(g["dos_peak_limit"]), filtering_iteration_limit=1)
+    w = _solve(g, s)
+    np.testing.assert_array_equal(s.last_mask.cpu().numpy(), [True, False, False, True, True])
+    _check(w, g, "filtered")
+    # the filter runs while solve_call_count < filtering_iteration_limit
+    assert s.solve_call_count == 1
+    s.last_mask = None
+    _solve(g, s)
+    assert s.last_mask is None
+
+
+def test_w_solve_batches_and_containers(cuda_device, fixture):
+    """Energy batches of two and DSDBCOO containers (small blocks in,
+    superblocks out) give the same W."""
+    g = fixture
+    ref = _solve(g, _solver(g, cuda_device, filtering_iteration_limit=0))
+    ns, b = g["v_diag"].shape[0], g["v_diag"].shape[-1]
+    ne = g["energies"].size
+    rows, cols = [], []
+    for i in range(ns):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < ns:
+                r, c = np.meshgrid(np.arange(b) + i * b, np.arange(b) + j * b, indexing="ij")
+                rows.append(r.ravel())
+                cols.append(c.ravel())
+    import scipy.sparse as sps
+
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    pattern = sps.coo_matrix((np.ones(rows.size, dtype=np.complex128), (rows, cols)), shape=(ns * b, ns * b))
+
+    def container(k, stack):
+        m = DSDBCOO.from_sparray(pattern, np.full(ns, b), stack, device=cuda_device)
+        d, u, lo = _bt(g, k)
+        for i in range(ns):
+            m.blocks[i, i] = torch.as_tensor(np.broadcast_to(d[i], stack + (b, b)).copy())
+            if i + 1 < ns:
+                m.blocks[i, i + 1] = torch.as_tensor(np.broadcast_to(u[i], stack + (b, b)).copy())
+                m.blocks[i + 1, i] = torch.as_tensor(np.broadcast_to(lo[i], stack + (b, b)).copy())
+        return m
+
+    nc = int(g["num_connected_blocks"])
+    s = CoulombScreeningSolve(container("v", (1,)), nc, g["energies"], filtering_iteration_limit=0,
+                              max_batch_size=2, device=cuda_device)
+    w = s.solve(container("p_lesser", (ne,)), container("p_greater", (ne,)),
+                container("p_retarded_hermitian", (ne,)))
+    for a, r in zip(w, ref):
+        for t in range(3):
+            assert _rel(torch.stack(a[t]).cpu().numpy(), torch.stack(r[t]).cpu().numpy()) < 1e-12
