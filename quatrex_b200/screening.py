@@ -37,7 +37,7 @@ import numpy as np
 import torch
 
 from . import _native
-from ._interop import default_device, mat, to_device
+from ._interop import default_device, from_device, mat, to_device
 from ._native import NULL_MAT, QtxBT, QtxMat
 from .lyapunov import Doubling, LyapunovSystem, screened_contact_obc
 from .obc import OBCSystem, SanchoRubio, _stream
@@ -308,11 +308,12 @@ class CoulombScreeningSolve:
         self.solve_call_count += 1
         if out is not None:
             for container, ww in zip(out, w):
+                like = container.data
                 for i in range(ns):
-                    container.blocks[i, i] = ww[0][i]
+                    container.blocks[i, i] = from_device(ww[0][i], like)
                     if i + 1 < ns:
-                        container.blocks[i, i + 1] = ww[1][i]
-                        container.blocks[i + 1, i] = ww[2][i]
+                        container.blocks[i, i + 1] = from_device(ww[1][i], like)
+                        container.blocks[i + 1, i] = from_device(ww[2][i], like)
         return w[0], w[1]
 
     def _filter_peaks(self, w):

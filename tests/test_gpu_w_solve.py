@@ -70,7 +70,7 @@ def test_w_solve_peak_filter_matches_reference(cuda_device, fixture):
 
 def test_w_solve_batches_and_containers(cuda_device, fixture):
     """Energy batches of two and DSDBCOO containers (small blocks in,
-    superblocks out) give the same W."""
+    superblocks out, written through ``out=``) give the same W."""
     g = fixture
     ref = _solve(g, _solver(g, cuda_device, filtering_iteration_limit=0))
     ns, b = g["v_diag"].shape[0], g["v_diag"].shape[-1]
@@ -100,8 +100,21 @@ def test_w_solve_batches_and_containers(cuda_device, fixture):
     nc = int(g["num_connected_blocks"])
     s = CoulombScreeningSolve(container("v", (1,)), nc, g["energies"], filtering_iteration_limit=0,
                               max_batch_size=2, device=cuda_device)
+    nsup, nb = ns // nc, nc * b
+    sup = np.zeros((ns * b, ns * b))
+    for i in range(nsup):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < nsup:
+                sup[i * nb:(i + 1) * nb, j * nb:(j + 1) * nb] = 1.0
+    outs = tuple(DSDBCOO.from_sparray(sps.coo_matrix(sup.astype(np.complex128)), np.full(nsup, nb), (ne,),
+                                      device=cuda_device) for _ in range(2))
     w = s.solve(container("p_lesser", (ne,)), container("p_greater", (ne,)),
-                container("p_retarded_hermitian", (ne,)))
-    for a, r in zip(w, ref):
+                container("p_retarded_hermitian", (ne,)), out=outs)
+    for a, r, o in zip(w, ref, outs):
         for t in range(3):
             assert _rel(torch.stack(a[t]).cpu().numpy(), torch.stack(r[t]).cpu().numpy()) < 1e-12
+        for i in range(nsup):
+            torch.testing.assert_close(o.blocks[i, i], a[0][i], rtol=0, atol=0)
+            if i + 1 < nsup:
+                torch.testing.assert_close(o.blocks[i, i + 1], a[1][i], rtol=0, atol=0)
+                torch.testing.assert_close(o.blocks[i + 1, i], a[2][i], rtol=0, atol=0)
