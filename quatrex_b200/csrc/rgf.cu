@@ -366,9 +366,12 @@ int solve_impl(const SolveIO& io, int64_t batch, int* info, Workspace& ws, cudaS
   // Forward sweep (rgf.py:241-302). The retarded chain runs on the helper
   // stream `sr`; the lesser/greater products of block j wait for the inverse
   // of block j, and the helper reuses the buffer of P (double-buffered by the
-  // parity of j) only after the products of block j - 2 are done. Not with
-  // the int8-emulated products, whose digit-plane scratch is shared.
-  const bool use_side = N > 1 && !(gemm_slices() > 0 && oz_bound(nullptr) != nullptr);
+  // parity of j) only after the products of block j - 2 are done. Only for
+  // batches below the SM count (at full batches the inverse occupies every
+  // SM and the products would only share SMs with it), and not with the
+  // int8-emulated products, whose digit-plane scratch is shared.
+  const bool use_side =
+      N > 1 && batch < (int64_t)num_sms() && !(gemm_slices() > 0 && oz_bound(nullptr) != nullptr);
   SideStream* ss = nullptr;
   cudaStream_t sr = s;
   if (use_side) {
