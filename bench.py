@@ -62,9 +62,11 @@ def parse():
                         "products emulated on the int8 tensor cores from this many digit planes (0: skip). "
                         "5 (default) is the fastest setting inside the transmission-error target of 1e-6; "
                         "6 gives FP64-class accuracy (the library default)")
-    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels"], default="cfg1",
+    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels", "inverse"], default="cfg1",
                    help="cfg1 (default): the headline line. cfg2: 64 blocks of 512x512, mixed vs FP64. "
-                        "cfg3: eight uneven devices on one GPU. cfg4: the serving loop.")
+                        "cfg3: eight uneven devices on one GPU. cfg4: the serving loop. inverse: the batched "
+                        "inverse of --batch blocks of --block-size on the selected --inverse-path")
+    p.add_argument("--block-size", type=int, default=256, help="block size of the inverse workload")
     p.add_argument("--cfg3-energies", type=int, default=32, help="energies per device of the uneven batch")
     p.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the resident solvers")
     p.add_argument("--cfg4-catalogue", choices=["small", "cfg3"], default="small",
@@ -982,6 +984,49 @@ def run_cfg4(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_inverse(args, local):
+    """The batched complex128 inverse alone (qtx_zinv_batched_ws, the call the
+    RGF and Sancho-Rubio drivers make): --batch blocks of --block-size,
+    diagonally shifted random matrices, inputs resident, CUDA-event timed
+    over --steps launches after --warmup."""
+    import ctypes
+
+    import torch
+
+    from quatrex_b200 import _native
+    from quatrex_b200._interop import mat
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    lib = _native.load()
+    n, B = args.block_size, args.batch
+    g = torch.Generator(device=device).manual_seed(0)
+    a = (torch.randn((B, n, n), dtype=torch.complex128, device=device, generator=g)
+         + n * torch.eye(n, dtype=torch.complex128, device=device))
+    x = torch.empty_like(a)
+    info = torch.zeros(B, dtype=torch.int32, device=device)
+    ws = torch.empty(lib.qtx_zinv_workspace(n, B), dtype=torch.uint8, device=device)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def launch():
+        _native.check(lib.qtx_zinv_batched_ws(n, B, mat(a), mat(x), info.data_ptr(), ws.data_ptr(), ws.numel(),
+                                              stream))
+
+    for _ in range(max(args.warmup, 3)):
+        launch()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.steps):
+        launch()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / args.steps
+    print(json.dumps({"metric": "batched inverse (complex flops 8n^3)", "unit": "TFLOP/s",
+                      "value": 8.0 * n ** 3 * B / (ms * 1e-3) / 1e12, "ms_per_launch": ms, "block_size": n,
+                      "batch": B, "inverse_path": args.inverse_path, "steps": args.steps}), flush=True)
+
+
 def run_kernels(args, local):
     """Kernel-level rooflines at the cfg1 block shape: batched complex GEMMs
     (ours and cuBLAS through torch on the same shapes) and batched inverses
@@ -1131,7 +1176,8 @@ def main():
     _native.check(_native.load().qtx_set_inverse_path({"auto": 0, "single": 1, "wide": 2, "cluster": 3, "split": 4}[args.inverse_path]))
     if args.workload != "cfg1":
         if rank == 0:
-            {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels}[args.workload](args, local)
+            {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels,
+             "inverse": run_inverse}[args.workload](args, local)
         return
     run_ours(args, world, rank, local)
 
