@@ -27,7 +27,8 @@ namespace qtx {
 // doubles the number of correct bits; then 1 / z = conj(z') (1 / m) 2^-e.
 // A few ulps from the correctly rounded quotient, like Smith's algorithm,
 // with one short dependency chain instead of three divisions.
-__device__ __forceinline__ z64 gj_recip(z64 z) {
+// gj_recip_scaled: the same with frexp / ldexp (any exponent, zero, subnormals).
+__device__ __forceinline__ z64 gj_recip_scaled(z64 z) {
   const double mx = fmax(fabs(z.x), fabs(z.y));
   if (mx == 0.0) return make_double2(0.0, 0.0);
   int e;
@@ -39,6 +40,25 @@ __device__ __forceinline__ z64 gj_recip(z64 z) {
 #pragma unroll
   for (int it = 0; it < 3; ++it) y = fma(y, fma(-m, y, 1.0), y);
   return make_double2(ldexp(xs * y, -e), ldexp(-ys * y, -e));
+}
+
+// gj_recip: for exponents away from the ends of the range the scale 2^-e is
+// built from the exponent field and applied by multiplication (exact, and
+// the final product rounds like ldexp), which keeps frexp / ldexp off the
+// pivot row's critical path; bit-identical to gj_recip_scaled.
+__device__ __forceinline__ z64 gj_recip(z64 z) {
+  const double mx = fmax(fabs(z.x), fabs(z.y));
+  const int eb = (int)((__double_as_longlong(mx) >> 52) & 0x7FF);  // biased exponent field
+  if (eb < 24 || eb > 2000) return gj_recip_scaled(z);             // zero, subnormal or extreme
+  const int e = eb - 1022;                                         // frexp's exponent of mx
+  const double s = __longlong_as_double((long long)(1023 - e) << 52);  // 2^-e
+  const double xs = z.x * s, ys = z.y * s;
+  const double m = fma(xs, xs, ys * ys);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(m));
+#pragma unroll
+  for (int it = 0; it < 3; ++it) y = fma(y, fma(-m, y, 1.0), y);
+  return make_double2((xs * y) * s, (-ys * y) * s);
 }
 
 __device__ __forceinline__ double gj_abs1(z64 z) { return fabs(z.x) + fabs(z.y); }
