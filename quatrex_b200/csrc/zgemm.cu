@@ -134,16 +134,18 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
     const z64* Ag = at<const z64>(d.A, b);
     const z64* Bg = at<const z64>(d.B, b);
 
-    double acc_re[MT][NT][4];
-    double acc_im[MT][NT][4];
+    // 3M (Gauss) products: p1 = sum ar br, p2 = sum ai bi,
+    // p3 = sum (ar + ai)(br + bi); Re = p1 - p2, Im = p3 - p1 - p2.
+    double p1[MT][NT][4], p2[MT][NT][4], p3[MT][NT][4];
 #pragma unroll
     for (int i = 0; i < MT; ++i)
 #pragma unroll
       for (int j = 0; j < NT; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          acc_re[i][j][q] = 0.0;
-          acc_im[i][j][q] = 0.0;
+          p1[i][j][q] = 0.0;
+          p2[i][j][q] = 0.0;
+          p3[i][j][q] = 0.0;
         }
 
     // Prologue.
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
       const z64* bs = Bs + (kt % STAGES) * B_SIZE;
 #pragma unroll
       for (int kk = 0; kk < BK; kk += 4) {
-        double ar[MT][2], ai[MT][2], nai[MT][2];
+        double ar[MT][2], ai[MT][2], sa[MT][2];
 #pragma unroll
         for (int i = 0; i < MT; ++i) {
           const int r = wm0 + i * 16 + g;
@@ -188,10 +190,10 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
           ar[i][1] = v1.x;
           ai[i][0] = (OPA == 1) ? -v0.y : v0.y;
           ai[i][1] = (OPA == 1) ? -v1.y : v1.y;
-          nai[i][0] = -ai[i][0];
-          nai[i][1] = -ai[i][1];
+          sa[i][0] = ar[i][0] + ai[i][0];
+          sa[i][1] = ar[i][1] + ai[i][1];
         }
-        double br[NT], bi[NT];
+        double br[NT], bi[NT], sb[NT];
 #pragma unroll
         for (int j = 0; j < NT; ++j) {
           const int c = wn0 + j * 8 + g;
@@ -202,23 +204,22 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
             v = bs[(kk + tq) * (BN + 2) + c];
           br[j] = v.x;
           bi[j] = (OPB == 1) ? -v.y : v.y;
+          sb[j] = br[j] + bi[j];
         }
-        // Two passes over the 2x4 tiles so that the two products feeding one
-        // accumulator are 16 independent MMAs apart (no dependent issue).
+        // Three passes over the 2x4 tiles: the products feeding one
+        // accumulator are 8 independent MMAs apart.
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
-          for (int j = 0; j < NT; ++j) {
-            mma_f64(acc_re[i][j], ar[i][0], ar[i][1], br[j]);
-            mma_f64(acc_im[i][j], ar[i][0], ar[i][1], bi[j]);
-          }
+          for (int j = 0; j < NT; ++j) mma_f64(p1[i][j], ar[i][0], ar[i][1], br[j]);
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
-          for (int j = 0; j < NT; ++j) {
-            mma_f64(acc_re[i][j], nai[i][0], nai[i][1], bi[j]);
-            mma_f64(acc_im[i][j], ai[i][0], ai[i][1], br[j]);
-          }
+          for (int j = 0; j < NT; ++j) mma_f64(p2[i][j], ai[i][0], ai[i][1], bi[j]);
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) mma_f64(p3[i][j], sa[i][0], sa[i][1], sb[j]);
       }
     }
     cp_async_wait<0>();
@@ -237,7 +238,9 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
         for (int q = 0; q < 4; ++q) {
           const int rl = wm0 + i * 16 + g + ((q >> 1) << 3);
           const int cl = wn0 + j * 8 + 2 * tq + (q & 1);
-          tile[rl * TS + cl] = zmul(d.alpha, make_double2(acc_re[i][j][q], acc_im[i][j][q]));
+          const double re = p1[i][j][q] - p2[i][j][q];
+          const double im = p3[i][j][q] - (p1[i][j][q] + p2[i][j][q]);
+          tile[rl * TS + cl] = zmul(d.alpha, make_double2(re, im));
         }
     for (int t = 0; t < d.nadd; ++t) {
       const Addend& ad = d.add[t];
