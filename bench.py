@@ -62,10 +62,11 @@ def parse():
                         "products emulated on the int8 tensor cores from this many digit planes (0: skip). "
                         "5 (default) is the fastest setting inside the transmission-error target of 1e-6; "
                         "6 gives FP64-class accuracy (the library default)")
-    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels", "inverse"], default="cfg1",
+    p.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "kernels", "inverse", "w"], default="cfg1",
                    help="cfg1 (default): the headline line. cfg2: 64 blocks of 512x512, mixed vs FP64. "
                         "cfg3: eight uneven devices on one GPU. cfg4: the serving loop. inverse: the batched "
-                        "inverse of --batch blocks of --block-size on the selected --inverse-path")
+                        "inverse of --batch blocks of --block-size on the selected --inverse-path. w: the "
+                        "screened-interaction (W) solve of a Coulomb-screening step")
     p.add_argument("--block-size", type=int, default=256, help="block size of the inverse workload")
     p.add_argument("--cfg3-energies", type=int, default=32, help="energies per device of the uneven batch")
     p.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the resident solvers")
@@ -989,6 +990,76 @@ def run_cfg4(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_w(args, local):
+    """The screened-interaction (W) solve of a Coulomb-screening step
+    (CoulombScreeningSolver.solve): 24 small blocks of 128 in superblocks of
+    three (8 superblocks of 384), 64 energies per step in batches of 32,
+    synthetic polarizations (quatrex_b200.synthetic.screened_device).
+    GPU energy-points/s (CUDA events over --steps solves after --warmup),
+    the oracle's restatement of the reference on the host cores on a
+    2-energy sample beside it, and the assembly / selected-solve flops."""
+    import torch
+
+    from oracle import negf_oracle as o
+    from quatrex_b200 import synthetic
+    from quatrex_b200.negf import flops_per_energy
+    from quatrex_b200.screening import CoulombScreeningSolve
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    ns, b, nc, ne = 24, 128, 3, 64
+    d = synthetic.screened_device(ns, b, ne, seed=7)
+    energies = np.linspace(0.05, 1.0, ne)
+
+    def dev(t):
+        return tuple([torch.from_numpy(np.ascontiguousarray(x)).to(device) for x in lst] for lst in t)
+
+    pl, pg, prh = dev(d["p_lesser"]), dev(d["p_greater"]), dev(d["p_retarded_hermitian"])
+    solver = CoulombScreeningSolve(d["v"], nc, energies, filtering_iteration_limit=0, max_batch_size=32,
+                                   device=device)
+    for _ in range(max(args.warmup, 1)):
+        solver.solve(pl, pg, prh)
+    torch.cuda.synchronize()
+    gpu = str(getattr(torch.cuda.get_device_properties(device), "uuid", ""))
+    clocks = ClockSampler(gpu if gpu.startswith("GPU-") else "GPU-" + gpu if gpu else "0")
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        solver.solve(pl, pg, prh)
+    t1.record()
+    torch.cuda.synchronize()
+    sec = t0.elapsed_time(t1) * 1e-3
+    clk = clocks.stop()
+    value = args.steps * ne / sec
+    # as-written flops per energy: the small-block products of M and L (9 + 2 x 24
+    # per block row, 8 b^3 each) and the selected solve on the superblocks
+    n_sup, bs = ns // nc, nc * b
+    fl = (9 + 48) * ns * 8.0 * b ** 3 + flops_per_energy(n_sup, bs)["solve"]
+    cpu = None
+    if not args.no_cpu:
+        import os
+        import time
+
+        sub = lambda lst: [x[:2] for x in lst]  # noqa: E731
+        args_cpu = [tuple(sub(lst) for lst in d[k]) for k in ("p_lesser", "p_greater", "p_retarded_hermitian")]
+        t = time.perf_counter()
+        o.w_solve(d["v"], *args_cpu, nc, energies[:2], lambda x: o.obc_system_solve(x[0], x[1], x[2], 100, 1e-12)[0],
+                  lambda bb, q: o.lyapunov_system_solve(bb, q)[0])
+        cs = time.perf_counter() - t
+        cpu = {"value": 2 / cs, "unit": "energy-points/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "2 energies of the 64 (one batch)", "seconds": cs}
+    print(json.dumps({
+        "metric": "W energy-points/s (Coulomb-screening step)", "value": value, "unit": "energy-points/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "higher_is_better": True, "dtype": "f64 (complex128)", "data": "synthetic",
+        "config": {"workload": f"{ns} small blocks of {b} in superblocks of {nc} ({n_sup} of {bs}), {ne} energies "
+                               "per step in batches of 32: P^R assembly, I - V P^R and V P^< V, V P^> V with the "
+                               "contact spillover, Lyapunov boundary conditions, selected solve"},
+        "as_written_tflops": value * fl / 1e12, "flops_per_energy": fl, "cpu_baseline": cpu, "clocks": clk}),
+        flush=True)
+
+
 def run_inverse(args, local):
     """The batched complex128 inverse alone (qtx_zinv_batched_ws, the call the
     RGF and Sancho-Rubio drivers make): --batch blocks of --block-size,
@@ -1182,7 +1253,7 @@ def main():
     if args.workload != "cfg1":
         if rank == 0:
             {"cfg2": run_cfg2, "cfg3": run_cfg3, "cfg4": run_cfg4, "kernels": run_kernels,
-             "inverse": run_inverse}[args.workload](args, local)
+             "inverse": run_inverse, "w": run_w}[args.workload](args, local)
         return
     run_ours(args, world, rank, local)
 
