@@ -86,6 +86,19 @@ int qtx_zgemm_batched(int m, int n, int k, int64_t batch, double alpha_re, doubl
                       qtx_mat a, int op_a, qtx_mat b, int op_b, double beta_re, double beta_im,
                       qtx_mat d, int op_d, qtx_mat c, qtx_stream stream);
 
+/* Grouped form of qtx_zgemm_batched: entry b reads op(A) at a_ptrs[b],
+ * op(B) at b_ptrs[b], D at d_ptrs[b] (NULL table: no addend) and writes C at
+ * c_ptrs[b]; row strides lda, ldb, ldd, ldc are shared. The tables are
+ * device arrays of `batch` device pointers, each 16-byte aligned; entries may
+ * share operands (a broadcast block) and D may equal C (accumulation).
+ * k > 0; always the FP64 DMMA products. The batched block products of the
+ * reference's bd_matmul / bd_sandwich (qttools/datastructures/
+ * routines.py:8-102,354-467) in one launch per band. */
+int qtx_zgemm_grouped(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                      const void* const* a_ptrs, int64_t lda, int op_a, const void* const* b_ptrs, int64_t ldb,
+                      int op_b, double beta_re, double beta_im, const void* const* d_ptrs, int64_t ldd, int op_d,
+                      void* const* c_ptrs, int64_t ldc, qtx_stream stream);
+
 /* Batched complex64 GEMM on the tcgen05 tensor cores, split-TF32 products
  * with FP32 accumulation (mixed precision path):
  * C = alpha op(A) op(B) + beta op(D), complex64 interleaved. err: optional

@@ -53,6 +53,9 @@ SIGNATURES = {
     "qtx_cgemm_batched": (c_int, [c_int, c_int, c_int, c_int64, ctypes.c_float, ctypes.c_float, QtxMat, c_int,
                                   QtxMat, c_int, ctypes.c_float, ctypes.c_float, QtxMat, c_int, QtxMat, c_void_p,
                                   c_void_p]),
+    "qtx_zgemm_grouped": (c_int, [c_int, c_int, c_int, c_int64, c_double, c_double, c_void_p, c_int64, c_int,
+                                  c_void_p, c_int64, c_int, c_double, c_double, c_void_p, c_int64, c_int, c_void_p,
+                                  c_int64, c_void_p]),
     "qtx_zcombine": (c_int, [c_int, c_int, c_int64, QtxMat, c_int, POINTER(QtxMat), POINTER(c_double),
                              c_void_p, c_void_p]),
     "qtx_zinv_batched": (c_int, [c_int, c_int64, QtxMat, QtxMat, c_void_p, c_void_p]),

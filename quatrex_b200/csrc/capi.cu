@@ -436,6 +436,42 @@ int qtx_selected_solve_mixed(const qtx_bt* a, const qtx_bt* sigma_lesser,
   });
 }
 
+int qtx_zgemm_grouped(int m, int n, int k, int64_t batch, double alpha_re, double alpha_im,
+                      const void* const* a_ptrs, int64_t lda, int op_a, const void* const* b_ptrs, int64_t ldb,
+                      int op_b, double beta_re, double beta_im, const void* const* d_ptrs, int64_t ldd, int op_d,
+                      void* const* c_ptrs, int64_t ldc, qtx_stream stream) {
+  return guarded([&] {
+    if (m < 0 || n < 0 || k <= 0 || batch < 0 || (op_a != 0 && op_a != 1) || (op_b != 0 && op_b != 1) ||
+        (op_d != 0 && op_d != 1) || a_ptrs == nullptr || b_ptrs == nullptr || c_ptrs == nullptr || lda <= 0 ||
+        ldb <= 0 || ldc <= 0 || (d_ptrs != nullptr && ldd <= 0)) {
+      set_error("qtx_zgemm_grouped: invalid arguments");
+      return (int)QTX_ERR_ARG;
+    }
+    GemmDesc g;
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.batch = batch;
+    // the tables stand in for the base pointers (non-null, 16-byte aligned)
+    g.A = MatRef{const_cast<void*>(static_cast<const void*>(a_ptrs)), lda, 0};
+    g.B = MatRef{const_cast<void*>(static_cast<const void*>(b_ptrs)), ldb, 0};
+    g.C = MatRef{const_cast<void*>(static_cast<const void*>(c_ptrs)), ldc, 0};
+    g.opA = op_a;
+    g.opB = op_b;
+    g.alpha = make_double2(alpha_re, alpha_im);
+    g.a_ptrs = reinterpret_cast<const z64* const*>(a_ptrs);
+    g.b_ptrs = reinterpret_cast<const z64* const*>(b_ptrs);
+    g.c_ptrs = reinterpret_cast<z64* const*>(c_ptrs);
+    if (d_ptrs != nullptr) {
+      g.add[0] = Addend{MatRef{const_cast<void*>(static_cast<const void*>(d_ptrs)), ldd, 0},
+                        make_double2(beta_re, beta_im), op_d};
+      g.nadd = 1;
+      g.d_ptrs = reinterpret_cast<const z64* const*>(d_ptrs);
+    }
+    return zgemm(g, (cudaStream_t)stream);
+  });
+}
+
 int qtx_zcombine(int m, int n, int64_t batch, qtx_mat out, int nterms, const qtx_mat* terms,
                  const double* coefs, const int* conj_trans, qtx_stream stream) {
   return guarded([&] {

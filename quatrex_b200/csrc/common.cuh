@@ -106,6 +106,13 @@ struct GemmDesc {
   MatRef C3;
   z64 scale3{1.0, 0.0};
   const int* active = nullptr;  // optional per-batch mask (0 = skip entry)
+  // Grouped form (DMMA path only): device tables of per-entry pointers that
+  // replace base + b * stride of A, B, the first addend and C (row strides
+  // from the MatRefs); no C2 / C3.
+  const z64* const* a_ptrs = nullptr;
+  const z64* const* b_ptrs = nullptr;
+  const z64* const* d_ptrs = nullptr;
+  z64* const* c_ptrs = nullptr;
 };
 
 int zgemm(const GemmDesc& d, cudaStream_t s);

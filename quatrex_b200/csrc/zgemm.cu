@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
 
   for (int64_t b = blockIdx.z; b < d.batch; b += gridDim.z) {
     if (d.active != nullptr && d.active[b] == 0) continue;
-    const z64* Ag = at<const z64>(d.A, b);
-    const z64* Bg = at<const z64>(d.B, b);
+    const z64* Ag = d.a_ptrs ? d.a_ptrs[b] : at<const z64>(d.A, b);
+    const z64* Bg = d.b_ptrs ? d.b_ptrs[b] : at<const z64>(d.B, b);
 
     // 3M (Gauss) products: p1 = sum ar br, p2 = sum ai bi,
     // p3 = sum (ar + ai)(br + bi); Re = p1 - p2, Im = p3 - p1 - p2.
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
     for (int t = 0; t < d.nadd; ++t) {
       const Addend& ad = d.add[t];
       if (!ad.conj_trans) continue;
-      const z64* p = at<const z64>(ad.m, b);
+      const z64* p = (t == 0 && d.d_ptrs) ? d.d_ptrs[b] : at<const z64>(ad.m, b);
       z64 x[MT][NT][4];  // all loads first: many in flight, no aliasing stalls
 #pragma unroll
       for (int i = 0; i < MT; ++i)
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
     for (int t = 0; t < d.nadd; ++t) {
       const Addend& ad = d.add[t];
       if (ad.conj_trans) continue;
-      const z64* p = at<const z64>(ad.m, b);
+      const z64* p = (t == 0 && d.d_ptrs) ? d.d_ptrs[b] : at<const z64>(ad.m, b);
       z64 x[PER];  // all loads first: many in flight, no aliasing stalls
 #pragma unroll
       for (int k = 0; k < PER; ++k) {
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_kernel(const KernelArgs args
       }
     }
     if (!d.C.null()) {
-      z64* out = at<z64>(d.C, b);
+      z64* out = d.c_ptrs ? d.c_ptrs[b] : at<z64>(d.C, b);
 #pragma unroll 8
       for (int e = tid; e < BM * BN; e += THREADS) {
         const int rl = e / BN, cl = e % BN;
@@ -358,7 +358,14 @@ int zgemm(const GemmDesc& d, cudaStream_t s) {
     set_error("zgemm: invalid sizes or addend count");
     return QTX_ERR_ARG;
   }
-  if (d.K > 0 && (d.A.null() || d.B.null())) {
+  const bool grouped = d.a_ptrs || d.b_ptrs || d.c_ptrs || d.d_ptrs;
+  if (grouped && (d.K <= 0 || !d.a_ptrs || !d.b_ptrs || !d.c_ptrs || d.nadd > 1 || d.nadd3 > 0 ||
+                  (d.nadd == 1 && !d.d_ptrs) || !d.C2.null() || !d.C3.null())) {
+    set_error("zgemm: the grouped form needs A, B and C tables, K > 0, at most one addend (with its table) "
+              "and no second outputs");
+    return QTX_ERR_ARG;
+  }
+  if (!grouped && d.K > 0 && (d.A.null() || d.B.null())) {
     // A zero operand: the product vanishes; only the addends remain.
     GemmDesc z = d;
     z.K = 0;
@@ -372,7 +379,7 @@ int zgemm(const GemmDesc& d, cudaStream_t s) {
     return QTX_ERR_ARG;
   }
   GemmDesc dd = d;
-  for (int t = 0; t < d.nadd + d.nadd3; ++t) {
+  for (int t = 0; !grouped && t < d.nadd + d.nadd3; ++t) {
     if (dd.add[t].m.null()) {  // drop zero addends
       for (int u = t; u + 1 < dd.nadd + dd.nadd3; ++u) dd.add[u] = dd.add[u + 1];
       if (t < dd.nadd)
@@ -388,7 +395,7 @@ int zgemm(const GemmDesc& d, cudaStream_t s) {
     if (dd.A.null()) dd.A = dd.C.null() ? dd.C3 : dd.C;
     if (dd.B.null()) dd.B = dd.A;
   }
-  if (dd.K > 0 && gemm_slices() > 0 && oz_supported(dd.K, gemm_slices())) {
+  if (!grouped && dd.K > 0 && gemm_slices() > 0 && oz_supported(dd.K, gemm_slices())) {
     size_t bytes = 0;
     void* scr = oz_bound(&bytes);
     if (scr != nullptr) return zgemm_oz(dd, gemm_slices(), scr, bytes, s);

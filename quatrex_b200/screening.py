@@ -60,6 +60,49 @@ def _bt_lists(x, n, device):
     return [dev(t) for t in diag], [dev(t) for t in upper], [dev(t) for t in lower]
 
 
+class _Grouped:
+    """Grouped GEMM launches (``qtx_zgemm_grouped``) of b x b blocks: every
+    launch is a list of (A, B, C) device addresses with C (+)= alpha A B; the
+    pointer tables of all launches go to the device in one copy, then the
+    launches run in the order they were added."""
+
+    def __init__(self, b: int, device: torch.device):
+        self.b, self.device = b, device
+        self.launches = []  # (alpha, accumulate, lda, ldb, ldc, a, b, c)
+
+    def add(self, alpha, accumulate, lda, ldb, ldc, a, bb, c):
+        """a, bb, c: lists of int64 address arrays (concatenated in order)."""
+        if a:
+            self.launches.append((alpha, accumulate, lda, ldb, ldc, np.concatenate(a), np.concatenate(bb),
+                                  np.concatenate(c)))
+
+    def run(self):
+        if not self.launches:
+            return
+        lib = _native.load()
+        tables, offs = [], []
+        pos = 0
+        for *_, a, bb, c in self.launches:
+            n = len(a)
+            pad = n + (n & 1)  # each table starts 16-byte aligned
+            for t in (a, bb, c):
+                offs.append(pos)
+                tables.append(t)
+                if pad > n:
+                    tables.append(np.zeros(1, dtype=np.int64))
+                pos += pad
+        dev = torch.from_numpy(np.concatenate(tables)).to(self.device)
+        base = dev.data_ptr()
+        stream = _stream(self.device)
+        for li, (alpha, acc, lda, ldb, ldc, a, bb, c) in enumerate(self.launches):
+            pa, pb, pc = (base + 8 * offs[3 * li + t] for t in range(3))
+            _native.check(lib.qtx_zgemm_grouped(self.b, self.b, self.b, len(a), alpha, 0.0, pa, lda, 0, pb, ldb, 0,
+                                                1.0 if acc else 0.0, 0.0, pc if acc else None, ldc, 0, pc, ldc,
+                                                stream))
+        self._keep = dev  # the tables live until the launches have run (stream order)
+        self.launches = []
+
+
 class CoulombScreeningSolve:
     """GPU W solve for one rank (``CoulombScreeningSolver.solve``).
 
@@ -177,14 +220,39 @@ class CoulombScreeningSolve:
                 terms = (QtxMat * 3)(mat(x_h), mat(x_g), mat(x_l))
                 _native.check(lib.qtx_zcombine(b, b, batch, mat(o), 3, terms, coefs, None, stream))
                 pr[t].append(o)
-        # M = I - V P^R - spillover, in superblocks (solver.py:542-578)
+        nb = self.nc * b
+        es = np.arange(batch, dtype=np.int64)
+        zb = b * b * 16  # bytes per small block of one energy
+
+        def a_v(i, j):  # an energy-independent V block, broadcast over the batch
+            return np.full(batch, self._v(i, j).data_ptr(), dtype=np.int64)
+
+        def a_blk(t):  # the energies of a (batch, b, b) stack
+            return t.data_ptr() + es * zb
+
+        def a_quad(sup, i, j):  # small block (i, j) of its superblock, every energy
+            return self._quad(sup, i, j).data_ptr() + es * (nb * nb * 16)
+
+        # M = I - V P^R - spillover, in superblocks (solver.py:542-578): one
+        # grouped launch per (k - i, j - i) over all block rows and energies,
+        # k ascending for every output block as bd_matmul sums it
         msup = self._superblocks(batch, identity=True)
-        for i in range(n):
-            for j in range(max(i - 2, 0), min(i + 3, n)):
-                for k in range(i - 1, i + 2):
-                    if abs(j - k) > 1 or k < 0 or k >= n:
-                        continue
-                    self._gemm(self._v(i, k), blk(pr, k, j), self._quad(msup, i, j), alpha=-1.0)
+        grp = _Grouped(b, dev)
+        for dk in (-1, 0, 1):
+            for dj in range(dk - 1, dk + 2):
+                if abs(dj) > 2:
+                    continue
+                A, B_, C = [], [], []
+                for i in range(n):
+                    k, j = i + dk, i + dj
+                    # blocks outside the superblock tridiagonal band (only for
+                    # nc < 3) are not read by the selected solve: skipped
+                    if 0 <= k < n and 0 <= j < n and abs(i // self.nc - j // self.nc) <= 1:
+                        A.append(a_v(i, k))
+                        B_.append(a_blk(blk(pr, k, j)))
+                        C.append(a_quad(msup, i, j))
+                grp.add(-1.0, True, b, b, nb, A, B_, C)
+        grp.run()
         self._gemm(self._v(1, 0), blk(pr, 0, 1), self._quad(msup, 0, 0), alpha=-1.0)
         self._gemm(self._v(n - 2, n - 1), blk(pr, n - 1, n - 2), self._quad(msup, n - 1, n - 1), alpha=-1.0)
         # contact boundary self-energies (solver.py:380-446)
@@ -210,25 +278,34 @@ class CoulombScreeningSolve:
             obc[side] = (r, lo, g)
         # L = V P V with the spillover (solver.py:823-838, 580-678)
         lsup = []
+        tmp = torch.empty((n, 5, batch, b, b), dtype=_C128, device=dev)  # ab[i][k - i + 2]
         for p_ in (pl, pg):
             sup = self._superblocks(batch)
-            tmp = [torch.empty((batch, b, b), dtype=_C128, device=dev) for _ in range(5)]
-            for i in range(n):
-                filled = [False] * 5  # ab[k] for k = i - 2 .. i + 2
-                for m in range(i - 1, i + 2):
-                    if m < 0 or m >= n:
-                        continue
-                    for k in range(m - 1, m + 2):
-                        if k < 0 or k >= n:
-                            continue
-                        s = k - i + 2
-                        self._gemm(self._v(i, m), blk(p_, m, k), tmp[s], accumulate=filled[s])
-                        filled[s] = True
-                for j in range(max(i - 3, 0), min(i + 4, n)):
-                    for k in range(j - 1, j + 2):
-                        if k < 0 or k >= n or abs(k - i) > 2 or not filled[k - i + 2]:
-                            continue
-                        self._gemm(tmp[k - i + 2], self._v(k, j), self._quad(sup, i, j))
+            tmp.zero_()
+            # ab[i][k] = sum over m (ascending) of V[i, m] P[m, k]
+            grp = _Grouped(b, dev)
+            for dm in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    A, B_, C = [], [], []
+                    for i in range(n):
+                        m, k = i + dm, i + dm + dk
+                        if 0 <= m < n and 0 <= k < n:
+                            A.append(a_v(i, m))
+                            B_.append(a_blk(blk(p_, m, k)))
+                            C.append(a_blk(tmp[i, k - i + 2]))
+                    grp.add(1.0, True, b, b, b, A, B_, C)
+            # L[i, j] = sum over k (ascending) of ab[i][k] V[k, j]
+            for dj in range(-3, 4):
+                for dkj in (-1, 0, 1):
+                    A, B_, C = [], [], []
+                    for i in range(n):
+                        j, k = i + dj, i + dj + dkj
+                        if 0 <= j < n and 0 <= k < n and abs(k - i) <= 2 and abs(i // self.nc - j // self.nc) <= 1:
+                            A.append(a_blk(tmp[i, k - i + 2]))
+                            B_.append(a_v(k, j))
+                            C.append(a_quad(sup, i, j))
+                    grp.add(1.0, True, b, b, nb, A, B_, C)
+            grp.run()
             t1 = torch.empty((batch, b, b), dtype=_C128, device=dev)
             for (a0, a1) in ((0, 1), (n - 1, n - 2)):
                 # left: v10 = V[1,0], v01 = V[0,1]; right: the flipped-order blocks
@@ -240,7 +317,7 @@ class CoulombScreeningSolve:
                     self._gemm(t1, z, self._quad(sup, i, j))
             lsup.append(sup)
         # selected solve on the superblocks (solver.py:843-864)
-        ns, nb = n // self.nc, self.nc * b
+        ns = n // self.nc
         keep = []
 
         def bt(diag, upper, lower):

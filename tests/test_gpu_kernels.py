@@ -47,6 +47,38 @@ def test_zgemm_matches_numpy(cuda_device, m, n, k, op_a, op_b):
     assert err < 1e-14 * max(1.0, np.sqrt(k)), err
 
 
+@pytest.mark.parametrize("op_a,op_b", [(0, 0), (1, 0), (0, 1)])
+def test_zgemm_grouped_matches_numpy(cuda_device, op_a, op_b):
+    """qtx_zgemm_grouped: per-entry pointers from device tables, a broadcast
+    A block (the same pointer in two entries), accumulation into C (D = C) and
+    a plain store; against NumPy."""
+    rng = np.random.default_rng(31 + op_a * 2 + op_b)
+    b, lib = 24, _native.load()
+    X = torch.from_numpy(_rand(rng, 5, b, b)).to(cuda_device)
+    C0 = _rand(rng, 3, b, b)
+    Y = torch.from_numpy(C0).to(cuda_device)
+    stride = b * b * 16
+    tab = lambda addrs: torch.tensor(addrs, dtype=torch.int64, device=cuda_device)  # noqa: E731
+    pa = tab([X.data_ptr(), X.data_ptr(), X.data_ptr() + stride])
+    pb = tab([X.data_ptr() + 2 * stride, X.data_ptr() + 3 * stride, X.data_ptr() + 4 * stride])
+    pc = tab([Y.data_ptr() + e * stride for e in range(3)])
+    x = X.cpu().numpy()
+    a_idx, b_idx = [0, 0, 1], [2, 3, 4]
+    _native.check(lib.qtx_zgemm_grouped(b, b, b, 3, 0.5, -1.0, pa.data_ptr(), b, op_a, pb.data_ptr(), b, op_b,
+                                        1.0, 0.0, pc.data_ptr(), b, 0, pc.data_ptr(), b, _stream()))
+    ref = np.stack([C0[e] + (0.5 - 1j) * (_op(x[a_idx[e]], op_a) @ _op(x[b_idx[e]], op_b)) for e in range(3)])
+    got = Y.cpu().numpy()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-14
+    # plain store (no addend table)
+    _native.check(lib.qtx_zgemm_grouped(b, b, b, 3, 1.0, 0.0, pa.data_ptr(), b, op_a, pb.data_ptr(), b, op_b,
+                                        0.0, 0.0, None, 0, 0, pc.data_ptr(), b, _stream()))
+    ref = np.stack([_op(x[a_idx[e]], op_a) @ _op(x[b_idx[e]], op_b) for e in range(3)])
+    assert np.linalg.norm(Y.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-14
+    with pytest.raises(_native.QtxError):
+        _native.check(lib.qtx_zgemm_grouped(b, b, 0, 3, 1.0, 0.0, pa.data_ptr(), b, 0, pb.data_ptr(), b, 0, 0.0,
+                                            0.0, None, 0, 0, pc.data_ptr(), b, _stream()))
+
+
 def test_zgemm_zero_k_and_null_operand(cuda_device):
     rng = np.random.default_rng(5)
     d = _rand(rng, 2, 8, 8)
