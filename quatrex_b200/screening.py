@@ -55,6 +55,7 @@ def _bt_lists(x, n, device):
         lower = [x.blocks[i + 1, i] for i in range(n - 1)]
     else:
         diag, upper, lower = x
+
     def dev(t):
         return to_device(t, device).to(_C128).contiguous()
     return [dev(t) for t in diag], [dev(t) for t in upper], [dev(t) for t in lower]
@@ -364,6 +365,15 @@ class CoulombScreeningSolve:
         pg = _bt_lists(p_greater, n, dev)
         prh = _bt_lists(p_retarded_hermitian, n, dev)
         ne = pl[0][0].shape[0]
+        for name, m in (("p_lesser", pl), ("p_greater", pg), ("p_retarded_hermitian", prh)):
+            counts = (len(m[0]), len(m[1]), len(m[2]))
+            if counts != (n, n - 1, n - 1):
+                raise ValueError(f"{name}: expected {n} diagonal and {n - 1} off-diagonal blocks, got {counts}")
+            for lst in m:
+                for x in lst:
+                    if tuple(x.shape) != (ne, self.b, self.b):
+                        raise ValueError(f"{name}: blocks must be ({ne}, {self.b}, {self.b}) stacks, got "
+                                         f"{tuple(x.shape)}")
         ns, nb = n // self.nc, self.nc * self.b
         w = []
         for _ in range(2):

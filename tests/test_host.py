@@ -80,3 +80,22 @@ def test_flop_model():
     assert abs(f["solve"] / 1e9 - 142.1) < 0.1
     assert abs(f["current"] / 1e9 - 38.0) < 0.1
     assert f["sr"] == 2 * u * (11 * 20 + 1)
+
+
+def test_w_solve_validates_block_counts():
+    """The W solve rejects polarizations whose block structure does not match
+    the Coulomb matrix before anything reaches the GPU (the constructor only
+    needs the Coulomb blocks; checked without a device by a CPU-side stub)."""
+    import numpy as np
+    import pytest
+
+    from quatrex_b200.screening import CoulombScreeningSolve
+
+    s = CoulombScreeningSolve.__new__(CoulombScreeningSolve)
+    s.num_small, s.b, s.nc, s.device = 6, 4, 3, "cpu"
+    blocks = ([np.zeros((2, 4, 4))] * 6, [np.zeros((2, 4, 4))] * 5, [np.zeros((2, 4, 4))] * 4)
+    with pytest.raises(ValueError, match="off-diagonal"):
+        s.solve(blocks, blocks, blocks)
+    bad = ([np.zeros((2, 4, 4))] * 6, [np.zeros((2, 4, 4))] * 5, [np.zeros((2, 4, 3))] * 5)
+    with pytest.raises(ValueError, match="stacks"):
+        s.solve(bad, bad, bad)
