@@ -192,9 +192,13 @@ int qtx_selected_inv(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt*
  * before anything is enqueued or written. All calls share the array: calls
  * that overlap on the GPU race. A device's first call resolves the array's
  * device address; make it before any stream capture. It always runs the FP64
- * DMMA products and the one-CTA-per-block inverse: the thread's GEMM path
- * (qtx_set_gemm_path) and qtx_set_inverse_path do not apply to it. This entry
- * point has no counterpart in the reference. */
+ * DMMA products (the thread's GEMM path, qtx_set_gemm_path, does not apply)
+ * and only the inverses that need no scratch: one CTA per block, the same
+ * kernel column-split over a thread-block cluster, or one cluster per block
+ * in distributed shared memory, chosen as for qtx_zinv_batched (including
+ * qtx_set_inverse_path); the multi-CTA panel inverse (mode 2, or the automatic
+ * choice for blocks above 400 at small batches) is replaced by one CTA per
+ * block. This entry point has no counterpart in the reference. */
 int qtx_selected_inv_static(const qtx_bt* a, const qtx_mat* obc_retarded, const qtx_bt* x,
                             int64_t batch, int* info, qtx_stream stream);
 
