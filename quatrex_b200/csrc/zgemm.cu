@@ -7,12 +7,13 @@
 // warp-level DMMA (mma.sync m16n8k4 .f64) -- on B200 the FP64 tensor and
 // vector rates are equal, and DMMA needs 8x fewer issue slots than DFMA.
 //
-// Complex arithmetic uses the 4M split on interleaved operands: one 16-byte
-// shared-memory load yields the real and the imaginary fragment of an
-// element, and  Re += Ar Br - Ai Bi,  Im += Ar Bi + Ai Br  are four real
-// MMAs sharing fragments. Conjugate-transposed operands are staged k-major
-// so every fragment load stays conflict-free (strides = 4 mod 8 or 2 mod 8
-// in 16-byte units), and conjugation is a compile-time sign flip.
+// Complex arithmetic uses the 3M (Gauss) form on interleaved operands: one
+// 16-byte shared-memory load yields the real and the imaginary fragment of an
+// element, and the three real MMAs  Ar Br,  Ai Bi  and  (Ar + Ai)(Br + Bi)
+// give  Re = p1 - p2  and  Im = p3 - p1 - p2  in the epilogue.
+// Conjugate-transposed operands are staged k-major so every fragment load
+// stays conflict-free (strides = 4 mod 8 or 2 mod 8 in 16-byte units), and
+// conjugation is a compile-time sign flip.
 //
 // Tiles: CTA 64x64 complex, 4 warps of 32x32, BK = 8 complex per stage,
 // 4-stage cp.async pipeline (zero-filled at the matrix edges). The epilogue
