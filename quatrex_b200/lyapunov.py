@@ -214,20 +214,24 @@ def screened_contact_obc(p_retarded, p_lesser, p_greater, v, obc, lyapunov, cont
     m_10_x_00 = _mm(m_10, x_00)
     obc_retarded = _mm(m_10_x_00, m_01)
 
-    def sandwich_sum(terms):
-        """sum of v_a @ p @ v_b, accumulated on the GPU."""
-        acc = None
-        for va, pp, vb in terms:
-            t = _mm(va, pp)
-            acc = _zgemm(t, vb, torch.empty_like(p00), addend=acc)
-        return acc
-
     def l_superblocks(p_):  # solver.py:307-335
+        """l_00 = sum of the 7 and l_01 of the 5 products v_a q v_b the
+        reference lists, grouped by the left Coulomb factor:
+        l_00 = v10 s1 + v00 s3 + v01 s4 and l_01 = v10 q01 v01 + v00 s1 + v01 s2
+        with the inner sums s1 = q00 v01 + q01 v00, s2 = q10 v01 + q00 v00,
+        s3 = s2 + q01 v10 and s4 = q10 v00 + q00 v10, which both blocks share:
+        14 batched products instead of 24."""
         q10, q00, q01 = (d3(x) for x in p_)
-        l_00 = sandwich_sum([(v10, q00, v01), (v10, q01, v00), (v00, q10, v01), (v00, q00, v00),
-                             (v00, q01, v10), (v01, q10, v00), (v01, q00, v10)])
-        l_01 = sandwich_sum([(v10, q01, v01), (v00, q00, v01), (v00, q01, v00), (v01, q10, v01),
-                             (v01, q00, v00)])
+
+        def e():
+            return torch.empty_like(p00)
+
+        s1 = _zgemm(q01, v00, e(), addend=_mm(q00, v01))
+        s2 = _zgemm(q00, v00, e(), addend=_mm(q10, v01))
+        s3 = _zgemm(q01, v10, e(), addend=s2)
+        s4 = _zgemm(q00, v10, e(), addend=_mm(q10, v00))
+        l_00 = _zgemm(v01, s4, e(), addend=_zgemm(v00, s3, e(), addend=_mm(v10, s1)))
+        l_01 = _zgemm(v01, s2, e(), addend=_zgemm(v00, s1, e(), addend=_mm(v10, _mm(q01, v01))))
         return l_00, l_01
 
     out = []
